@@ -1,0 +1,339 @@
+#!/usr/bin/env python
+"""Throughput of the D3Q19 LES time step on one B200 (or N replicas).
+
+Workload: the 512x256x256 arm case (simlab_b200.cases.arm_les): regularized
+D3Q19 with Smagorinsky LES Cs=0.17, Re 1e5 on the arm width, Bouzidi walls,
+wind-tunnel faces with sponges and absorbing layers.  A step is one lattice
+time step over all 33.5 M cells (faces, wall cells with the fused FP64
+force reduction, bulk collide-stream).
+
+Metric: MLUPS (all lattice cells x steps / s, as crates/cfd/examples/bench.rs)
+for FP16-stored populations (the headline `value`), beside the same engine's
+FP32 and BF16 storage and their fraction of the measured HBM copy bandwidth.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank runs its own replica of
+the case: the step has no data exchange across replicas ("replicas only").
+--impl reference times the reference's update restated on the CPU (the
+oracle; the reference itself is Rust + wgpu/Metal and cannot run here) on
+bounded samples of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "MLUPS (D3Q19 LES arm 512x256x256, FP16-stored populations)"
+UNIT = "MLUPS"
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profile(storage_name: str):
+    """DRAM bytes per k_bulk launch from the committed ncu summary, if any."""
+    f = ROOT / "profiles" / f"k_bulk_{storage_name}_arm_512x256x256.md"
+    if not f.exists():
+        return None
+    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", f.read_text())
+    return float(m.group(1)) if m else None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, n in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(v: float, ws: int) -> float:
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def time_storage(storage, steps, warmup, ws, with_profile):
+    """Device time of `steps` resident time steps, CUDA events on the lattice's stream."""
+    import torch
+
+    from simlab_b200.cases import arm_les
+    from simlab_b200.lbm import Lattice
+
+    st, vox = arm_les(storage)
+    lat = Lattice(st, vox)
+    stream = torch.cuda.ExternalStream(lat.stream)
+    lat.advance(warmup)
+    lat.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if with_profile:
+        lat.profile(True)
+    barrier(ws)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(stream):
+        e0.record()
+    lat.advance(steps)
+    with torch.cuda.stream(stream):
+        e1.record()
+    lat.synchronize()
+    torch.cuda.synchronize()
+    barrier(ws)
+    ms = e0.elapsed_time(e1)
+    kt = lat.kernel_times() if with_profile else None
+    if with_profile:
+        lat.profile(False)
+    mass, bad = lat.mass()
+    info = {"cells": st.cells(), "nrec": lat.nrec, "nface": lat.nface, "mass": mass, "nonfinite": bad}
+    return lat, ms, kt, info
+
+
+def e2e_time(lat, steps):
+    """Through the C-ABI call a caller makes (lbm_run with host buffers): per
+    step the StepIn goes host->device with the launch and the step's force
+    and moment come back to the host."""
+    from simlab_b200.lbm import STEP_DTYPE, steps_array
+
+    one = steps_array(1)
+    lat.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        f = lat.run(one)
+    t1 = time.perf_counter()
+    assert np.all(np.isfinite(f))
+    return (t1 - t0) * 1e3, STEP_DTYPE.itemsize, 6 * 8
+
+
+def cpu_sample(storage, sample_s: float = 12.0, warm: int = 1):
+    """The oracle (the reference's update restated in C++, OpenMP over all host
+    cores) on bounded samples of the same case: collide-stream over slabs of 8
+    z-planes of the full 512x256x256 lattice."""
+    import oracle
+    from simlab_b200.cases import arm_les
+
+    cores = oracle.set_threads(os.cpu_count() or 1)
+    st, vox = arm_les(storage)
+    lat = oracle.OracleLattice(st, vox)
+    nx, ny, nz = st.dims
+    slab = 8
+    for k in range(warm):
+        lat.step_slab(k * slab, (k + 1) * slab)
+    cells = 0
+    z = 0
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < sample_s:
+        lat.step_slab(z, z + slab)
+        cells += nx * ny * slab
+        z = (z + slab) % nz
+    dt = time.perf_counter() - t0
+    lat.close()
+    return cells / dt / 1e6, cores, f"{cells // (nx * ny * slab)} slabs of {nx}x{ny}x{slab} cells in {dt:.1f} s"
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    import oracle
+    from simlab_b200.cases import arm_les
+    from simlab_b200.lbm import Storage
+
+    cores = oracle.set_threads(os.cpu_count() or 1)
+    st, vox = arm_les(Storage.FP16)
+    lat = oracle.OracleLattice(st, vox)
+    nx, ny, nz = st.dims
+    slab = 2
+    for k in range(args.warmup):
+        lat.step_slab((k * slab) % nz, (k * slab) % nz + slab)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        z = (k * slab) % nz
+        lat.step_slab(z, z + slab)
+    dt = time.perf_counter() - t0
+    v = nx * ny * slab * args.steps / dt / 1e6
+    sample = f"each step: collide-stream over {nx}x{ny}x{slab} cells of the 512x256x256 arm lattice (FP16 storage)"
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / max(args.steps, 1), 3), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "D3Q19 LES arm 512x256x256 (oracle: the reference update restated in C++)", "storage": "fp16",
+                       "parallelism": "host threads"},
+            "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    ws, rank, local = dist_init()
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        return
+    import torch
+
+    from simlab_b200.cases import BYTES_PER_LUP
+    from simlab_b200.lbm import Storage
+
+    torch.cuda.set_device(local)
+    hbm, peak_kind = peaks()
+    results = {}
+    clocks = None
+    e2e = None
+    for storage in (Storage.FP16, Storage.FP32, Storage.BF16):
+        headline = storage == Storage.FP16
+        sampler = ClockSampler(local) if headline else None
+        if sampler:
+            sampler.start()
+        lat, ms, kt, info = time_storage(storage, args.steps, args.warmup, ws, with_profile=headline)
+        if sampler:
+            clocks = sampler.stop()
+        ms_max = max_over_ranks(ms, ws)
+        mlups = info["cells"] * args.steps * ws / (ms_max * 1e-3) / 1e6
+        r = {"mlups": mlups, "ms_per_step": ms_max / args.steps, "info": info}
+        if kt:
+            r["kernel_times"] = kt
+        if headline:
+            e_ms, hb, db = e2e_time(lat, args.steps)
+            e_ms = max_over_ranks(e_ms, ws)
+            e2e = {"value": round(info["cells"] * args.steps * ws / (e_ms * 1e-3) / 1e6, 3), "unit": UNIT, "h2d_bytes_per_step": hb,
+                   "d2h_bytes_per_step": db}
+        lat.close()
+        del lat
+        results[storage] = r
+        torch.cuda.synchronize()
+    h = results[Storage.FP16]
+    kt = h["kernel_times"]
+    bulk_ms = kt["bulk_ms"] / max(kt["steps"], 1)
+    cells = h["info"]["cells"]
+    alg_bytes = BYTES_PER_LUP[Storage.FP16] * cells
+    achieved = alg_bytes / (bulk_ms * 1e-3) / 1e9
+    traffic = traffic_from_profile("fp16")
+    line = {
+        "metric": METRIC,
+        "value": round(h["mlups"], 3),
+        "unit": UNIT,
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(h["ms_per_step"], 5),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32 arithmetic, fp16 storage",
+        "data": "synthetic",
+        "config": {"workload": "D3Q19 regularized + Smagorinsky LES (Cs 0.17), arm 200x12x8 + cylinder r10 h14, 512x256x256, "
+                               "u 0.05, Re 1e5, Bouzidi walls, wind-tunnel faces + sponges",
+                   "storage": "fp16 (f - w) x 32768, stochastic rounding", "parallelism": "replicas" if ws > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (1.41 GB of populations per replica)"},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                     "traffic": traffic, "kernel": "k_bulk<fp16>", "bytes_per_lup": BYTES_PER_LUP[Storage.FP16],
+                     "kernel_ms": round(bulk_ms, 5), "peak_source": peak_kind},
+        "storages": {s.name.lower(): {"mlups": round(r["mlups"], 3), "ms_per_step": round(r["ms_per_step"], 5),
+                                      "hbm_frac_step": round(BYTES_PER_LUP[s] * cells * r["mlups"] / cells / 1e3 / hbm, 4)}
+                     for s, r in results.items()},
+        "fp16_over_fp32": round(h["mlups"] / results[Storage.FP32]["mlups"], 3),
+        "clocks": clocks,
+        "e2e": e2e,
+        "gpu_launches": 3 * args.steps,
+        "kernel_share": {k: round(v / max(kt["faces_ms"] + kt["walls_ms"] + kt["bulk_ms"], 1e-12), 4) for k, v in kt.items() if k != "steps"},
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        v, cores, sample = cpu_sample(Storage.FP16)
+        line["cpu_baseline"] = {"value": round(v, 3), "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,259 @@
+/*
+ * simlab_lbm.h -- C ABI of the B200 lattice-Boltzmann engine.
+ *
+ * This is the boundary that replaces the lattice layer of SimLab's
+ * `crates/cfd` (the Rust `Lattice` type in crates/cfd/src/lattice.rs and the
+ * voxelizer entry points in crates/cfd/src/voxel.rs).  Each declaration names
+ * the reference item it stands in for.  Everything is in lattice units (cell
+ * size 1, time step 1, reference density 1), as in the reference.
+ *
+ * Conventions
+ *  - Every function returns an int status: 0 (LBM_OK) or a negative
+ *    lbm_status code.  The message of the last failure is available from
+ *    lbm_last_error() (per handle) or lbm_global_error() (creation errors).
+ *  - No exception or C++ type crosses the boundary; all arrays are plain host
+ *    memory owned by the caller, sizes are element counts.
+ *  - A handle is driven by one thread at a time (the reference drives a
+ *    `Lattice` from one job thread); it owns one CUDA stream.
+ *  - Cell index everywhere is (z * NY + y) * NX + x.
+ */
+#ifndef SIMLAB_LBM_H
+#define SIMLAB_LBM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_ABI_VERSION 1
+
+/* Status codes.  The reference returns anyhow::Result with bail! messages
+ * (e.g. lattice.rs:233-244, 414-419); the message text is kept in the handle. */
+typedef enum {
+    LBM_OK = 0,
+    LBM_ERR_INVALID = -1,     /* bad argument or setup (reference: bail!) */
+    LBM_ERR_NOMEM = -2,       /* device allocation failed (lattice.rs:417-419) */
+    LBM_ERR_CUDA = -3,        /* a CUDA call failed */
+    LBM_ERR_TIMEOUT = -4,     /* a device wait passed its host-side limit */
+    LBM_ERR_UNSUPPORTED = -5, /* feature not available for this configuration */
+    LBM_ERR_STATE = -6        /* call not valid in the handle's state (e.g. macros without debug_dump) */
+} lbm_status;
+
+/* Face boundary conditions, faces ordered -x, +x, -y, +y, -z, +z.
+ * VELOCITY/OPEN/PERIODIC mirror `FaceBc` (lattice.rs:35-43).  FREE_SLIP has
+ * no counterpart in the reference: the face cell holds the mirror image of
+ * its inner neighbour's post-collision populations (specular reflection). */
+typedef enum {
+    LBM_FACE_VELOCITY = 0,
+    LBM_FACE_OPEN = 1,
+    LBM_FACE_PERIODIC = 2,
+    LBM_FACE_FREE_SLIP = 3
+} lbm_face_bc;
+
+/* Population storage, `Storage` (lattice.rs:11-32) plus BF16 and FP64.
+ * All storage keeps f_i - w_i; FP16 scales it by 32768 with stochastic
+ * rounding (shader.rs:73, 507-517).  Arithmetic is FP32 except FP64. */
+typedef enum {
+    LBM_STORAGE_FP32 = 0,
+    LBM_STORAGE_FP16 = 1,
+    LBM_STORAGE_BF16 = 2,
+    LBM_STORAGE_FP64 = 3
+} lbm_storage;
+
+/* Collision operator.  REGULARIZED is the reference's (shader.rs:15-17,
+ * 835-837); BGK is plain single-relaxation BGK (no counterpart). */
+typedef enum {
+    LBM_COLLISION_REGULARIZED = 0,
+    LBM_COLLISION_BGK = 1
+} lbm_collision;
+
+/* `LatticeSetup` (lattice.rs:45-76), field for field, plus `collision`. */
+typedef struct {
+    uint32_t dims[3];
+    int32_t faces[6];          /* lbm_face_bc, -x,+x,-y,+y,-z,+z */
+    double nu;                 /* lattice kinematic viscosity; tau0 = 0.5 + 3 nu */
+    double smagorinsky;        /* C_s (0 = no turbulence model) */
+    double u_inf[3];
+    double u_init[3];
+    double body_force[3];      /* uniform acceleration (Guo forcing) */
+    uint32_t sponge[6];        /* viscosity sponge width per face, cells */
+    double sponge_tau;
+    double sponge_sigma;
+    int32_t absorb_velocity;
+    int32_t total_pressure_inlet;
+    int32_t storage;           /* lbm_storage */
+    int32_t collision;         /* lbm_collision */
+    double center[3];          /* moment reference point and spin centre */
+    int32_t debug_dump;        /* keep a buffer for lbm_macros() */
+    int32_t wall_model;        /* Spalding wall model in wall cells */
+} lbm_setup;
+
+/* `WallCell` (voxel.rs:328-335): a wall-adjacent fluid cell, its cut-link
+ * mask (bit i = direction i) and q per direction (1.0 where no wall). */
+typedef struct {
+    uint32_t cell;
+    uint32_t mask;
+    float q[27];
+} lbm_wall_cell;
+
+/* `Geometry` (lattice.rs:87-92).  kind 0 = None, 1 = Static. */
+typedef struct {
+    int32_t kind;
+    int32_t _pad;
+    const uint32_t *solid;     /* solid cell indices (StaticVoxels::solid) */
+    uint64_t nsolid;
+    const lbm_wall_cell *walls;/* StaticVoxels::walls */
+    uint64_t nwalls;
+} lbm_geometry;
+
+/* `SliceDef` (shader.rs:77-84). */
+typedef struct {
+    int32_t origin[3];
+    int32_t u[3];
+    int32_t v[3];
+    uint32_t nu;
+    uint32_t nv;
+} lbm_slice_def;
+
+/* `Probes` (lattice.rs:94-102).  verts: 6 doubles per vertex (position
+ * relative to the centre in body coordinates, then the unit normal). */
+typedef struct {
+    const double *verts;
+    uint64_t nvert;
+    const lbm_slice_def *slices;
+    uint64_t nslices;
+    double vertex_offset;
+} lbm_probes;
+
+/* `StepIn` (lattice.rs:104-113).  rot[r][c]: row-major 3x3, columns are the
+ * body axes in lattice coordinates; omega in rad per step. */
+typedef struct {
+    double rot[3][3];
+    double rot_prev[3][3];
+    double omega[3];
+    int32_t sample;
+    int32_t _pad;
+} lbm_step_in;
+
+/* Public fields of `Lattice` (lattice.rs:148-170). */
+typedef struct {
+    uint64_t steps_done;
+    uint32_t nrec;
+    uint32_t nface;
+    uint32_t npix;
+    uint32_t nvert;
+    uint64_t memory_bytes;
+    uint64_t cells;
+    int32_t storage;           /* storage actually used */
+    int32_t collision;
+} lbm_info;
+
+typedef struct lbm_lattice lbm_lattice;
+typedef struct lbm_voxels lbm_voxels;
+
+/* Library version string. */
+const char *lbm_version(void);
+
+/* Message of the last failure of a call that had no handle (creation,
+ * voxelizer).  Copies at most len-1 bytes and a terminating zero. */
+int lbm_global_error(char *buf, uint64_t len);
+
+/* Message of the last failure on this handle. */
+int lbm_last_error(const lbm_lattice *h, char *buf, uint64_t len);
+
+/* Lattice::max_cells (lattice.rs:221-227): largest grid this storage can
+ * hold by the layout alone (device memory budgets are the caller's). */
+uint64_t lbm_max_cells(int32_t storage);
+
+/* Lattice::new (lattice.rs:229-673): validates the setup, builds face list,
+ * records and flags, allocates device memory and writes the initial state
+ * (equilibrium at u_init).  `probes` may be NULL. */
+int lbm_create(const lbm_setup *setup, const lbm_geometry *geom, const lbm_probes *probes, lbm_lattice **out);
+
+/* Drop (frees every device buffer of the handle). */
+void lbm_destroy(lbm_lattice *h);
+
+/* Lattice::run (lattice.rs:699-753): advances n steps; forces_out receives
+ * 6 doubles per step, the force and the moment about `center` on the
+ * geometry after each step (lattice units).  Blocks until the forces are on
+ * the host; returns LBM_ERR_TIMEOUT if the device does not finish within the
+ * handle's wait limit (lbm_set_timeout). */
+int lbm_run(lbm_lattice *h, const lbm_step_in *steps, uint64_t n, double *forces_out);
+
+/* Enqueues n still steps (StepIn::still(false)) on the handle's stream and
+ * returns without waiting; the forces stay in device memory.  For timing the
+ * resident time step (no reference counterpart). */
+int lbm_advance(lbm_lattice *h, uint64_t n);
+
+/* The handle's CUDA stream (cudaStream_t), for event timing. */
+int lbm_stream(lbm_lattice *h, void **stream);
+
+/* Waits for the handle's stream with the wait limit. */
+int lbm_synchronize(lbm_lattice *h);
+
+/* Per-kernel device time of the steps enqueued while profiling is on,
+ * from CUDA events recorded around each kernel on the handle's stream (no
+ * reference counterpart; for the roofline figures).  Enabling clears the
+ * totals; lbm_kernel_times waits for the stream and returns them. */
+typedef struct {
+    uint64_t steps;
+    double faces_ms;
+    double walls_ms;
+    double bulk_ms;
+} lbm_kernel_times;
+int lbm_profile(lbm_lattice *h, int32_t enable);
+int lbm_get_kernel_times(lbm_lattice *h, lbm_kernel_times *out);
+
+/* Host-side limit on device waits, seconds (default 600). */
+int lbm_set_timeout(lbm_lattice *h, double seconds);
+
+/* Lattice::macros (lattice.rs:818-835): (rho, ux, uy, uz) of every cell,
+ * NaN for solid and face cells; needs debug_dump.  out: 4 * cells floats. */
+int lbm_macros(lbm_lattice *h, float *out);
+
+/* Lattice::records (lattice.rs:837-841): the wall records, 40 u32 words per
+ * record in the reference's layout (shader.rs:62-69).  out: cap_words u32. */
+int lbm_records(lbm_lattice *h, uint32_t *out, uint64_t cap_words);
+
+/* Lattice::reset_samples / vertex_means / slice_means (lattice.rs:785-816).
+ * vertex_means: nvert floats; slice_means: 4 floats per pixel. */
+int lbm_reset_samples(lbm_lattice *h);
+int lbm_vertex_means(lbm_lattice *h, float *out);
+int lbm_slice_means(lbm_lattice *h, float *out);
+
+/* Public fields of Lattice (lattice.rs:148-170). */
+int lbm_get_info(const lbm_lattice *h, lbm_info *out);
+
+/* Global mass and the non-finite count over all fluid cells, summed in
+ * FP64 on the device (no reference counterpart; the reference checks forces
+ * for NaN in tunnel.rs:1142-1144). */
+int lbm_mass(lbm_lattice *h, double *mass, uint64_t *nonfinite);
+
+/* Checkpoint: size in bytes of the state blob, then save/load it (all
+ * populations, records and the step counter).  No reference counterpart. */
+int lbm_state_size(const lbm_lattice *h, uint64_t *bytes);
+int lbm_save_state(lbm_lattice *h, void *buf, uint64_t bytes);
+int lbm_load_state(lbm_lattice *h, const void *buf, uint64_t bytes);
+
+/* voxelize_static / voxelize_static27 (voxel.rs:346-359, 361-490): solid
+ * cells and wall links of a closed triangle surface given in lattice
+ * coordinates.  lattice: 19 or 27.  The result is read with
+ * lbm_voxels_counts / lbm_voxels_copy and freed with lbm_voxels_free. */
+int lbm_voxelize_static(const double *verts, uint64_t nverts, const uint32_t *tris, uint64_t ntris,
+                        const uint32_t dims[3], int32_t lattice, lbm_voxels **out);
+int lbm_voxels_counts(const lbm_voxels *v, uint64_t *nsolid, uint64_t *nwalls);
+int lbm_voxels_copy(const lbm_voxels *v, uint32_t *solid, lbm_wall_cell *walls);
+void lbm_voxels_free(lbm_voxels *v);
+
+/* inside_grid (voxel.rs:73-95): inside test for every point of the grid
+ * origin + h * (i, j, k); out: dims[0]*dims[1]*dims[2] bytes (0/1). */
+int lbm_inside_grid(const double *verts, uint64_t nverts, const uint32_t *tris, uint64_t ntris,
+                    const double origin[3], double h, const uint32_t dims[3], uint8_t *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SIMLAB_LBM_H */

@@ -1,0 +1,143 @@
+"""TEST INFRASTRUCTURE -- the CPU oracle of the D3Q19 time step.
+
+A C++ restatement of SimLab's WGSL update (crates/cfd/src/shader.rs) and its
+driver (crates/cfd/src/lattice.rs), see d3q19_oracle.hpp.  Imported only by
+the tests, the smoke check and the bench's CPU baseline; never by the engine.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from .build import LIB, build_oracle
+
+_lib = None
+
+
+def library() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        build_oracle()
+        L = C.CDLL(str(LIB))
+        vp, u64 = C.c_void_p, C.c_ulonglong
+        L.orc_create.argtypes = [vp, vp, C.c_int]
+        L.orc_create.restype = vp
+        L.orc_destroy.argtypes = [vp]
+        L.orc_destroy.restype = None
+        L.orc_run.argtypes = [vp, vp, u64, vp]
+        L.orc_macros.argtypes = [vp, vp]
+        L.orc_step_slab.argtypes = [vp, C.c_uint, C.c_uint]
+        L.orc_nrec.argtypes = [vp]
+        L.orc_nrec.restype = u64
+        L.orc_nface.argtypes = [vp]
+        L.orc_nface.restype = u64
+        L.orc_records.argtypes = [vp, vp]
+        L.orc_flags.argtypes = [vp, vp]
+        L.orc_faces.argtypes = [vp, vp]
+        L.orc_raw.argtypes = [vp, vp]
+        L.orc_steps_done.argtypes = [vp]
+        L.orc_steps_done.restype = u64
+        L.orc_last_error.argtypes = [C.c_char_p, u64]
+        L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_f32_to_f16.argtypes = [C.c_float]
+        L.orc_f32_to_f16.restype = C.c_uint16
+        L.orc_f16_to_f32.argtypes = [C.c_uint16]
+        L.orc_f16_to_f32.restype = C.c_float
+        L.orc_f16_bits_ref.argtypes = [C.c_float]
+        L.orc_f16_bits_ref.restype = C.c_uint16
+        L.orc_f32_to_bf16.argtypes = [C.c_float]
+        L.orc_f32_to_bf16.restype = C.c_uint16
+        L.orc_sround16.argtypes = [C.c_float, C.c_uint32, C.c_uint32]
+        L.orc_sround16.restype = C.c_float
+        _lib = L
+    return _lib
+
+
+def set_threads(n: int) -> int:
+    return library().orc_set_threads(int(n))
+
+
+class OracleLattice:
+    """The oracle with the same constructor and readback as simlab_b200.Lattice.
+
+    real64=False: the reference's FP32 update; real64=True: the FP64 oracle
+    (use Storage.FP64 in the setup for FP64 storage)."""
+
+    def __init__(self, setup, geometry=None, real64: bool = False):
+        from simlab_b200.lbm import geometry_struct  # the C-ABI structs are shared
+
+        L = library()
+        self._L = L
+        self.setup = setup
+        cs = setup.to_c()
+        g, keep = geometry_struct(geometry)
+        h = L.orc_create(C.addressof(cs), C.addressof(g), int(real64))
+        del keep
+        if not h:
+            buf = C.create_string_buffer(1024)
+            L.orc_last_error(buf, 1024)
+            raise RuntimeError(buf.value.decode())
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.orc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def steps_done(self) -> int:
+        return int(self._L.orc_steps_done(self._h))
+
+    @property
+    def nrec(self) -> int:
+        return int(self._L.orc_nrec(self._h))
+
+    @property
+    def nface(self) -> int:
+        return int(self._L.orc_nface(self._h))
+
+    def run(self, steps) -> np.ndarray:
+        from simlab_b200.lbm import STEP_DTYPE, steps_array
+
+        a = steps if isinstance(steps, np.ndarray) and steps.dtype == STEP_DTYPE else steps_array(steps)
+        a = np.ascontiguousarray(a)
+        out = np.zeros((len(a), 6), dtype=np.float64)
+        self._L.orc_run(self._h, a.ctypes.data, len(a), out.ctypes.data)
+        return out
+
+    def step_slab(self, z0: int, z1: int) -> None:
+        """CPU-baseline timing: one step's collide-stream over z-planes [z0, z1)."""
+        self._L.orc_step_slab(self._h, int(z0), int(z1))
+
+    def macros(self) -> np.ndarray:
+        out = np.empty((self.setup.cells(), 4), dtype=np.float64)
+        self._L.orc_macros(self._h, out.ctypes.data)
+        return out
+
+    def records(self) -> np.ndarray:
+        out = np.zeros(max(self.nrec, 1) * 40, dtype=np.uint32)
+        self._L.orc_records(self._h, out.ctypes.data)
+        return out
+
+    def flags(self) -> np.ndarray:
+        out = np.zeros(self.setup.cells(), dtype=np.uint32)
+        self._L.orc_flags(self._h, out.ctypes.data)
+        return out
+
+    def faces(self) -> np.ndarray:
+        out = np.zeros(self.nface, dtype=np.uint32)
+        self._L.orc_faces(self._h, out.ctypes.data)
+        return out
+
+    def raw(self) -> np.ndarray:
+        out = np.zeros(19 * self.setup.cells(), dtype=np.float64)
+        self._L.orc_raw(self._h, out.ctypes.data)
+        return out.reshape(19, -1)

@@ -1,0 +1,78 @@
+"""Builds the engine library (libsimlab_lbm.so, sm_100a) in-tree with nvcc.
+
+The library is the product: CUDA kernels, the C++ host driver behind the C ABI
+of include/simlab_lbm.h and the host voxelizer.  It is compiled for sm_100a
+only and placed next to this file so it travels with the source tree.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+LIB = PKG / "libsimlab_lbm.so"
+
+CUDA_SOURCES = ["d3q19_kernels.cu", "lattice.cu"]
+CXX_SOURCES = ["voxel.cpp"]
+HEADERS = ["lbm_device.cuh", "lbm_kernels.h", "voxel.hpp"]
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-fopenmp", "-Xptxas", "-v"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _stale(target: Path, deps: list[Path]) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def _run(cmd: list[str], log: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    log.append(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError(f"build step failed: {' '.join(cmd[:3])} ...")
+
+
+def build_library(force: bool = False, verbose: bool = False) -> Path:
+    deps = [CSRC / s for s in CUDA_SOURCES + CXX_SOURCES + HEADERS] + [ROOT / "include" / "simlab_lbm.h", Path(__file__)]
+    if not force and not _stale(LIB, deps):
+        return LIB
+    objdir = PKG / "_build"
+    objdir.mkdir(exist_ok=True)
+    log: list[str] = []
+    objs = []
+    cc = nvcc()
+    for src in CUDA_SOURCES:
+        obj = objdir / (src + ".o")
+        _run([cc, *ARCH, *NVCC_FLAGS, "-I", str(ROOT / "include"), "-c", str(CSRC / src), "-o", str(obj)], log)
+        objs.append(str(obj))
+    for src in CXX_SOURCES:
+        obj = objdir / (src + ".o")
+        _run(["g++", "-O3", "-std=c++17", "-fPIC", "-fopenmp", "-c", str(CSRC / src), "-o", str(obj)], log)
+        objs.append(str(obj))
+    tmp = LIB.with_suffix(".so.tmp")
+    _run([cc, *ARCH, "-shared", "-o", str(tmp), *objs, "-Xcompiler", "-fopenmp", "-lgomp", "-lcudart"], log)
+    os.replace(tmp, LIB)
+    (objdir / "build.log").write_text("\n".join(log))
+    if verbose:
+        print("\n".join(log))
+    return LIB
+
+
+if __name__ == "__main__":
+    build_library(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    print(LIB)

@@ -1,0 +1,64 @@
+"""Frozen workloads (synthetic inputs with the benchmark configurations'
+shapes): geometry generators and lattice setups shared by the tests, the
+smoke check and the bench.
+
+* `sphere_re40`: 96x48x48, sphere r=6 at (24,24,24), velocity inlet u=0.04,
+  open (zero-gradient pressure) outlet, free-slip sides, Re 40 on the
+  diameter (nu = 0.012, tau = 0.536), halfway bounce-back, plain BGK.
+* `arm_les`: 512x256x256 D3Q19 with the reference's regularized collision
+  and Smagorinsky LES (Cs = 0.17), a 200x12x8-cell box beam with a cylinder
+  (r = 10, h = 14, axis z) at its +y end centred at (128,128,128), inlet
+  u = 0.05, Re = 1e5 on the 12-cell width (nu = 6e-6, tau0 = 0.500018), the
+  reference's wind-tunnel faces (velocity inlet holding the total pressure,
+  open outlet and sides; tunnel.rs:764-771) with sponges 16/32/16 cells,
+  sponge tau 1.0 and absorbing strength 0.1 (tunnel.rs:206-234, 1006-1007).
+  `scale=2` gives the 1024x512x512 arm.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .lbm import Collision, FaceBc, LatticeSetup, Storage, halfway, voxelize_static
+from .shapes import arm, sphere
+
+
+def sphere_re40(storage=Storage.FP32, collision=Collision.BGK, debug_dump=True):
+    dims = (96, 48, 48)
+    center = (24.0, 24.0, 24.0)
+    r, u, re = 6.0, 0.04, 40.0
+    v, t = sphere(list(center), r, 5)
+    vox = halfway(voxelize_static(v, t, list(dims)))
+    F = FaceBc
+    st = LatticeSetup(dims=list(dims), faces=[F.VELOCITY, F.OPEN, F.FREE_SLIP, F.FREE_SLIP, F.FREE_SLIP, F.FREE_SLIP], nu=u * 2 * r / re,
+                      u_inf=[u, 0.0, 0.0], u_init=[u, 0.0, 0.0], collision=collision, storage=storage, center=list(center),
+                      debug_dump=debug_dump)
+    return st, vox
+
+
+def sphere_cd(fx, u=0.04, r=6.0):
+    return np.asarray(fx) / (0.5 * u * u * np.pi * r * r)
+
+
+def arm_les(storage=Storage.FP16, scale: int = 1, debug_dump=False, dims=None):
+    dims = tuple(dims) if dims is not None else (512 * scale, 256 * scale, 256 * scale)
+    c = (dims[0] / 4.0, dims[1] / 2.0, dims[2] / 2.0)
+    v, t = arm(center=c, scale=scale)
+    vox = voxelize_static(v, t, list(dims))
+    u = 0.05
+    nu = u * 12.0 / 1e5
+    F = FaceBc
+    sp = [16 * scale, 32 * scale] + [16 * scale] * 4
+    st = LatticeSetup(dims=list(dims), faces=[F.VELOCITY, F.OPEN, F.OPEN, F.OPEN, F.OPEN, F.OPEN], nu=nu, smagorinsky=0.17,
+                      u_inf=[u, 0.0, 0.0], u_init=[u, 0.0, 0.0], sponge=sp, sponge_tau=1.0, sponge_sigma=0.1, absorb_velocity=False,
+                      total_pressure_inlet=True, storage=storage, center=list(c), debug_dump=debug_dump,
+                      collision=Collision.REGULARIZED)
+    return st, vox
+
+
+def arm_reference_area(scale: int = 1) -> float:
+    """Frontal area of the arm seen from +x (beam 200x8 plus the cylinder's 20x14 above/below it is inside)."""
+    return float((200 * 8 + 0) * scale * scale)
+
+
+# algorithmic bytes per lattice update: 19 populations read and written once plus the u32 flag word
+BYTES_PER_LUP = {Storage.FP32: 156, Storage.FP16: 80, Storage.BF16: 80, Storage.FP64: 308}

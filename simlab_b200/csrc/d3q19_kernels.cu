@@ -1,0 +1,646 @@
+// D3Q19 time-step kernels for sm_100a.
+//
+// One step of parity P (crates/cfd/src/lattice.rs:715-737 dispatch order):
+//   k_faces  -- face cells: rebuild the "previous" post-collision populations
+//               from the inner neighbour (shader.rs:630-687; gather and write
+//               fused, which is race free because a face cell's inner
+//               neighbour is never a face cell), plus free-slip faces.
+//   k_walls  -- wall-record cells: streaming + Bouzidi / moving-wall links +
+//               collision (shader.rs:795-862 with $WALLS$ 399-436), and the
+//               momentum-exchange force and moment summed in FP64 with warp
+//               shuffles, per block, then by the last block in a fixed order
+//               (replaces reduce1/reduce2, shader.rs:689-734).
+//   k_bulk   -- every other fluid cell: fused AA stream + collide.
+// k_walls and k_bulk touch disjoint cells; in the AA pattern every memory
+// slot is read and written by exactly one thread per step, so they need no
+// ordering between them.  The population layout is the reference's
+// slot-major SoA (shader.rs:147-152): direction d of cell n at d * N + n,
+// stored as f - w (FP32, FP64, FP16 x 32768 with stochastic rounding, BF16).
+#include <cstdio>
+#include <utility>
+
+#include "lbm_device.cuh"
+#include "lbm_kernels.h"
+
+namespace lbm {
+
+// ---------------------------------------------------------------- collision
+// Everything of shader.rs:815-847 after the wall links: moments, Smagorinsky
+// tau from |Pi_neq| (825-828), wall model, sponge (832-833), regularized or
+// plain BGK relaxation, absorbing layer (838-845), Guo forcing (442-455).
+template <class R>
+__device__ R wall_tau(const LatParams &p, const Consts<R> &k, uint32_t r, uint32_t mask, R pcx, R pcy, R pcz, R ux, R uy, R uz,
+                      R tau_les, const R *om) {
+    // Spalding wall model, shader.rs:540-597
+    R ns[3] = {0, 0, 0};
+#pragma unroll
+    for (int i = 1; i < 19; i++) {
+        if (mask & (1u << i)) {
+            R q = (R)rec_q(p.recs, r, i);
+            R w = i < 7 ? (R)(1.0 / 18.0) : (R)(1.0 / 36.0);
+            ns[0] = ns[0] + (R)CX(i) * w * ((R)1.5 - q);
+            ns[1] = ns[1] + (R)CY(i) * w * ((R)1.5 - q);
+            ns[2] = ns[2] + (R)CZ(i) * w * ((R)1.5 - q);
+        }
+    }
+    R nl = sqrt(ns[0] * ns[0] + ns[1] * ns[1] + ns[2] * ns[2]);
+    if (nl < (R)1e-6) return tau_les;
+    R nw[3] = {ns[0] / nl, ns[1] / nl, ns[2] / nl};
+    R yy = 2;
+#pragma unroll
+    for (int i = 1; i < 19; i++) {
+        if (mask & (1u << i)) {
+            R cn = (R)CX(i) * nw[0] + (R)CY(i) * nw[1] + (R)CZ(i) * nw[2];
+            if (cn > (R)0.3) {
+                R q = (R)rec_q(p.recs, r, i);
+                yy = min(yy, max(q, (R)0.02) * cn);
+            }
+        }
+    }
+    if (yy > (R)1.9) return tau_les;
+    R xw[3] = {pcx + yy * nw[0], pcy + yy * nw[1], pcz + yy * nw[2]};
+    R uwx = om[1] * xw[2] - om[2] * xw[1], uwy = om[2] * xw[0] - om[0] * xw[2], uwz = om[0] * xw[1] - om[1] * xw[0];
+    R rx = ux - uwx, ry = uy - uwy, rz = uz - uwz;
+    R un = rx * nw[0] + ry * nw[1] + rz * nw[2];
+    R tx = rx - un * nw[0], ty = ry - un * nw[1], tz = rz - un * nw[2];
+    R ut = sqrt(tx * tx + ty * ty + tz * tz);
+    R nu0 = (k.tau0 - (R)0.5) / (R)3;
+    if (ut < (R)1e-7) return tau_les;
+    const R kap = (R)0.41;
+    R eb = exp(-kap * (R)5.2);
+    R ust = sqrt(nu0 * ut / yy);
+    for (int it = 0; it < 12; it++) {
+        R up = ut / ust;
+        R yp = yy * ust / nu0;
+        R ku = min(kap * up, (R)30);
+        R eku = exp(ku);
+        R g = up + eb * (eku - (R)1 - ku - (R)0.5 * ku * ku - ku * ku * ku / (R)6) - yp;
+        R dgdup = (R)1 + eb * kap * (eku - (R)1 - ku - (R)0.5 * ku * ku);
+        R dg = dgdup * (-up / ust) - yy / nu0;
+        R step = g / dg;
+        ust = min(max(ust - step, (R)0.1 * ust), (R)10 * ust);
+        if (fabs(step) < (R)1e-5 * ust) break;
+    }
+    R nuw = ust * ust * yy / ut;
+    return max((R)0.5 + (R)3 * max(nuw, nu0), tau_les);
+}
+
+// One cell's update after its populations f are loaded (and wall links
+// applied).  Returns rho and u (the u written to wall records).
+template <class R, int COLL>
+__device__ __forceinline__ void relax(const LatParams &p, const Consts<R> &k, R *f, uint32_t x, uint32_t y, uint32_t z,
+                                      bool wall, uint32_t r, uint32_t mask, R pcx, R pcy, R pcz, const R *om, R &rho_o, R &ux_o,
+                                      R &uy_o, R &uz_o) {
+    const Moments<R> m = moments<R>(f);
+    const R rho = (R)1 + m.rho1;
+    const R ux = m.jx / rho + (R)0.5 * k.grav[0];
+    const R uy = m.jy / rho + (R)0.5 * k.grav[1];
+    const R uz = m.jz / rho + (R)0.5 * k.grav[2];
+    R pi[6];
+    pi_neq<R>(m, rho, ux, uy, uz, pi);
+    R tau = k.tau0;
+    if (p.les_on) {
+        R pp = pi[0] * pi[0] + pi[1] * pi[1] + pi[2] * pi[2] + (R)2 * (pi[3] * pi[3] + pi[4] * pi[4] + pi[5] * pi[5]);
+        R qn = sqrt((R)2 * pp);
+        tau = (R)0.5 * (k.tau0 + sqrt(k.tau0 * k.tau0 + (R)18 * k.smag2 * qn / rho));
+    }
+    if (wall && p.wall_model && mask != 0u) tau = wall_tau<R>(p, k, r, mask, pcx, pcy, pcz, ux, uy, uz, tau, om);
+    R sp = 0;
+    if (p.sponge_on) {
+        sp = sponge_at<R>(k, p, x, y, z);
+        if (sp > (R)0 && k.sponge_tau > tau) tau = tau + sp * sp * (k.sponge_tau - tau);
+    }
+    const R omg = (R)1 / tau;
+    const R usq = (R)1.5 * (ux * ux + uy * uy + uz * uz);
+    const bool absorb = p.sponge_on && sp > (R)0 && k.sigma > (R)0;
+    R atx = ux, aty = uy, atz = uz;
+    if (p.abs_u) { atx = k.u_inf[0]; aty = k.u_inf[1]; atz = k.u_inf[2]; }
+    const R ausq = (R)1.5 * (atx * atx + aty * aty + atz * atz);
+    const R sg = k.sigma * sp * sp;
+    const R tr = (pi[0] + pi[1] + pi[2]) * (R)(1.0 / 3.0);
+    R Gx = 0, Gy = 0, Gz = 0, uG = 0, fo = 0;
+    if (p.forcing) {
+        Gx = rho * k.grav[0]; Gy = rho * k.grav[1]; Gz = rho * k.grav[2];
+        uG = ux * Gx + uy * Gy + uz * Gz;
+        fo = (R)1 - (R)0.5 * omg;
+    }
+#pragma unroll
+    for (int i = 0; i < 19; i++) {
+        const R fe = feq_i<R>(i, m.rho1, rho, ux, uy, uz, usq);
+        R v;
+        if (COLL == 1) v = f[i] - omg * (f[i] - fe);                 // plain BGK
+        else v = fe + ((R)1 - omg) * fneq_i<R>(i, pi, tr);           // regularized
+        if (absorb) {
+            const R ft = feq_i<R>(i, (R)0, (R)1, atx, aty, atz, ausq);
+            v = v + sg * (ft - fe);
+        }
+        if (p.forcing) {
+            const R cu = cdot<R>(i, ux, uy, uz), cg = cdot<R>(i, Gx, Gy, Gz);
+            R t = fo * ((R)3 * (cg - uG) + (R)9 * cu * cg);
+            if (COLL != 1) t = t - (R)1.5 * ((R)1 - omg) * cg;
+            v = v + (R)WD(i) * t;
+        }
+        f[i] = v;
+    }
+    rho_o = rho; ux_o = ux; uy_o = uy; uz_o = uz;
+}
+
+// ---------------------------------------------------------------- bulk
+// Plain fluid cells (flag word 0): the hot loop.
+template <class S, int P, int COLL>
+__global__ void __launch_bounds__(BLOCK) k_bulk(const __grid_constant__ LatParams p, const __grid_constant__ StepParams s) {
+    using R = typename Pop<S>::real;
+    const uint32_t n = blockIdx.x * BLOCK + threadIdx.x;
+    if (n >= p.N) return;
+    if (p.flags[n] != 0u) return;
+    uint32_t x, y, z;
+    coords(p, n, x, y, z);
+    const Nb nb = make_nb(p, x, y, z);
+    R f[19];
+    load_in<S, P>(p, n, nb, f);
+    const Consts<R> &k = K<R>(p);
+    R rho, ux, uy, uz;
+    const R om0[3] = {0, 0, 0};
+    relax<R, COLL>(p, k, f, x, y, z, false, 0, 0, 0, 0, 0, om0, rho, ux, uy, uz);
+    store_out<S, P>(p, n, nb, f, s.seed);
+}
+
+// ---------------------------------------------------------------- walls
+// One thread per wall record.  A record whose cell is a fluid wall cell is
+// updated with its links (Bouzidi-Firdaouss-Lallemand interpolated
+// bounce-back with the moving-wall term and Galilean-invariant momentum
+// exchange, shader.rs:399-436) and its post-collision state saved to the
+// record (437-441, 848-860).  Every record's F and T enter the step's sum.
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <class S, int P, int COLL>
+__global__ void __launch_bounds__(BLOCK) k_walls(const __grid_constant__ LatParams p, const __grid_constant__ StepParams s) {
+    using R = typename Pop<S>::real;
+    const Consts<R> &k = K<R>(p);
+    const uint32_t r = blockIdx.x * BLOCK + threadIdx.x;
+    R Fo[3] = {0, 0, 0}, To[3] = {0, 0, 0};
+    if (r < p.nrec) {
+        const uint32_t cell = p.recs[r * RS + R_CELL];
+        const uint32_t fg = cell < p.N ? p.flags[cell] : 1u;
+        if ((fg & 3u) == 0u && (fg >> 2) == r + 1u) {
+            uint32_t x, y, z;
+            coords(p, cell, x, y, z);
+            const Nb nb = make_nb(p, x, y, z);
+            R f[19];
+            load_in<S, P>(p, cell, nb, f);
+            R fin[19];
+#pragma unroll
+            for (int i = 0; i < 19; i++) fin[i] = f[i];
+            const uint32_t mask = p.recs[r * RS + R_MASK];
+            const R pcx = (R)x - k.center[0], pcy = (R)y - k.center[1], pcz = (R)z - k.center[2];
+            R om[3];
+            if (sizeof(R) == 8) { om[0] = (R)s.omega_d[0]; om[1] = (R)s.omega_d[1]; om[2] = (R)s.omega_d[2]; }
+            else { om[0] = (R)s.omega[0]; om[1] = (R)s.omega[1]; om[2] = (R)s.omega[2]; }
+#pragma unroll
+            for (int i = 1; i < 19; i++) {
+                if (mask & (1u << i)) {
+                    const int o = OPP(i);
+                    const R w = (R)WD(i);
+                    const R q = max((R)rec_q(p.recs, r, i), (R)0.001);
+                    const R fpi = Rec<R>::fpost(p, r, i) + w;
+                    const R fpo = Rec<R>::fpost(p, r, o) + w;
+                    const R cx = (R)CX(i), cy = (R)CY(i), cz = (R)CZ(i);
+                    const R xwx = pcx + q * cx, xwy = pcy + q * cy, xwz = pcz + q * cz;
+                    const R uwx = om[1] * xwz - om[2] * xwy, uwy = om[2] * xwx - om[0] * xwz, uwz = om[0] * xwy - om[1] * xwx;
+                    const R cu = cx * uwx + cy * uwy + cz * uwz;
+                    R fb;
+                    if (q >= (R)0.5) fb = (fpi + ((R)2 * q - (R)1) * fpo - (R)6 * w * cu) / ((R)2 * q);
+                    else if ((mask & (1u << o)) == 0u) fb = (R)2 * q * fpi + ((R)1 - (R)2 * q) * (fin[i] + w) - (R)6 * w * cu;
+                    else fb = fpi - (R)6 * w * cu;
+                    f[o] = fb - w;
+                    const R flx = (cx - uwx) * fpi + (cx + uwx) * fb;
+                    const R fly = (cy - uwy) * fpi + (cy + uwy) * fb;
+                    const R flz = (cz - uwz) * fpi + (cz + uwz) * fb;
+                    Fo[0] += flx; Fo[1] += fly; Fo[2] += flz;
+                    To[0] += xwy * flz - xwz * fly;
+                    To[1] += xwz * flx - xwx * flz;
+                    To[2] += xwx * fly - xwy * flx;
+                }
+            }
+            R rho, ux, uy, uz;
+            relax<R, COLL>(p, k, f, x, y, z, true, r, mask, pcx, pcy, pcz, om, rho, ux, uy, uz);
+#pragma unroll
+            for (int i = 1; i < 19; i++) Rec<R>::set_fpost(p, r, i, f[i]);
+            Rec<R>::set_macro(p, r, 0, rho);
+            Rec<R>::set_macro(p, r, 1, ux);
+            Rec<R>::set_macro(p, r, 2, uy);
+            Rec<R>::set_macro(p, r, 3, uz);
+            if (p.moving) {
+                for (int a = 0; a < 3; a++) { Fo[a] += Rec<R>::ft(p, r, a); To[a] += Rec<R>::ft(p, r, 3 + a); }
+            }
+            for (int a = 0; a < 3; a++) { Rec<R>::set_ft(p, r, a, Fo[a]); Rec<R>::set_ft(p, r, 3 + a, To[a]); }
+            store_out<S, P>(p, cell, nb, f, s.seed);
+        } else {
+            for (int a = 0; a < 3; a++) { Fo[a] = Rec<R>::ft(p, r, a); To[a] = Rec<R>::ft(p, r, 3 + a); }
+        }
+    }
+    // FP64 sum: warp shuffle -> block -> last block over all block partials
+    __shared__ double sh[BLOCK / 32][6];
+    __shared__ bool last;
+    double v[6] = {(double)Fo[0], (double)Fo[1], (double)Fo[2], (double)To[0], (double)To[1], (double)To[2]};
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < 6; j++) v[j] = warp_sum(v[j]);
+    if (lane == 0)
+        for (int j = 0; j < 6; j++) sh[warp][j] = v[j];
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double t = 0;
+        for (int w = 0; w < BLOCK / 32; w++) t += sh[w][threadIdx.x];
+        p.partials[blockIdx.x * 8 + threadIdx.x] = t;
+        __threadfence();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t t = atomicAdd(p.ticket, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += BLOCK)
+        for (int j = 0; j < 6; j++) acc[j] += __ldcg(&p.partials[b * 8 + j]);
+#pragma unroll
+    for (int j = 0; j < 6; j++) acc[j] = warp_sum(acc[j]);
+    __syncthreads();
+    if (lane == 0)
+        for (int j = 0; j < 6; j++) sh[warp][j] = acc[j];
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double t = 0;
+        for (int w = 0; w < BLOCK / 32; w++) t += sh[w][threadIdx.x];
+        p.hist[s.slot * 8 + threadIdx.x] = t;
+    }
+    if (threadIdx.x == 0) *p.ticket = 0u;
+}
+
+// ---------------------------------------------------------------- faces
+template <class R, int M, int I>
+__device__ __forceinline__ void mirror_one(const R *g, R *f) {
+    constexpr int j = DIR((M & 1) ? -CX(I) : CX(I), (M & 2) ? -CY(I) : CY(I), (M & 4) ? -CZ(I) : CZ(I));
+    f[I] = g[j];
+}
+template <class R, int M, int... Is>
+__device__ __forceinline__ void mirror_all(const R *g, R *f, std::integer_sequence<int, Is...>) {
+    (mirror_one<R, M, Is>(g, f), ...);
+}
+template <class R, int M>
+__device__ __forceinline__ void mirror(const R *g, R *f) {
+    mirror_all<R, M>(g, f, std::make_integer_sequence<int, 19>{});
+}
+
+template <class S, int P>
+__global__ void __launch_bounds__(BLOCK) k_faces(const __grid_constant__ LatParams p, const __grid_constant__ StepParams s) {
+    using R = typename Pop<S>::real;
+    constexpr int Q = 1 - P;
+    const Consts<R> &k = K<R>(p);
+    const uint32_t kf = blockIdx.x * BLOCK + threadIdx.x;
+    if (kf >= p.nface) return;
+    const uint32_t b = p.faces[kf];
+    const uint32_t info = p.face_info[kf];
+    uint32_t x, y, z;
+    coords(p, b, x, y, z);
+    uint32_t cx = x, cy = y, cz = z;
+    if (!p.per[0]) cx = min(max(cx, 1u), p.NX - 2);
+    if (!p.per[1]) cy = min(max(cy, 1u), p.NY - 2);
+    if (!p.per[2]) cz = min(max(cz, 1u), p.NZ - 2);
+    const uint32_t m = (cz * p.NY + cy) * p.NX + cx;
+    const uint32_t fg = p.flags[m];
+    const Nb nbm = make_nb(p, cx, cy, cz);
+    R f[19];
+    if ((info & 3u) == 2u) {
+        // free slip: mirror image of the inner neighbour (no reference counterpart)
+        if ((fg & 3u) == 0u) {
+            R g[19];
+            load_prev_out<S, Q>(p, m, nbm, g);
+            switch (info >> 2) {
+                case 1: mirror<R, 1>(g, f); break;
+                case 2: mirror<R, 2>(g, f); break;
+                case 3: mirror<R, 3>(g, f); break;
+                case 4: mirror<R, 4>(g, f); break;
+                case 5: mirror<R, 5>(g, f); break;
+                case 6: mirror<R, 6>(g, f); break;
+                case 7: mirror<R, 7>(g, f); break;
+                default: mirror<R, 0>(g, f); break;
+            }
+        } else {
+            const R usq = (R)1.5 * (k.u_inf[0] * k.u_inf[0] + k.u_inf[1] * k.u_inf[1] + k.u_inf[2] * k.u_inf[2]);
+#pragma unroll
+            for (int i = 0; i < 19; i++) f[i] = feq_i<R>(i, (R)0, (R)1, k.u_inf[0], k.u_inf[1], k.u_inf[2], usq);
+        }
+    } else {
+        R rho = 1, ux = k.u_inf[0], uy = k.u_inf[1], uz = k.u_inf[2];
+        R pi[6] = {0, 0, 0, 0, 0, 0};
+        if ((fg & 3u) == 0u) {
+            R g[19];
+            load_prev_out<S, Q>(p, m, nbm, g);
+            const Moments<R> mo = moments<R>(g);
+            rho = (R)1 + mo.rho1;
+            ux = mo.jx / rho - (R)0.5 * k.grav[0];
+            uy = mo.jy / rho - (R)0.5 * k.grav[1];
+            uz = mo.jz / rho - (R)0.5 * k.grav[2];
+            pi_neq<R>(mo, rho, ux, uy, uz, pi);
+        }
+        if ((info & 3u) == 0u) {
+            if (p.total_p) {
+                const R uinf2 = k.u_inf[0] * k.u_inf[0] + k.u_inf[1] * k.u_inf[1] + k.u_inf[2] * k.u_inf[2];
+                rho = ((R)(1.0 / 3.0) + (R)0.5 * uinf2) / ((R)(1.0 / 3.0) + (R)0.5 * (ux * ux + uy * uy + uz * uz));
+            } else {
+                ux = k.u_inf[0]; uy = k.u_inf[1]; uz = k.u_inf[2];
+            }
+        } else {
+            rho = 1;
+        }
+        const R rho1 = rho - (R)1;
+        const R usq = (R)1.5 * (ux * ux + uy * uy + uz * uz);
+        const R tr = (pi[0] + pi[1] + pi[2]) * (R)(1.0 / 3.0);
+#pragma unroll
+        for (int i = 0; i < 19; i++) f[i] = feq_i<R>(i, rho1, rho, ux, uy, uz, usq) + fneq_i<R>(i, pi, tr);
+    }
+    const Nb nbb = make_nb(p, x, y, z);
+    store_prev_out<S, Q>(p, b, x, y, z, nbb, f, s.seed);
+}
+
+// ---------------------------------------------------------------- init
+// shader.rs:623-628: every cell holds the equilibrium at u_init (step seed 0)
+template <class S>
+__global__ void __launch_bounds__(BLOCK) k_init(const __grid_constant__ LatParams p) {
+    using R = typename Pop<S>::real;
+    const Consts<R> &k = K<R>(p);
+    const uint32_t n = blockIdx.x * BLOCK + threadIdx.x;
+    if (n >= p.N) return;
+    S *pop = (S *)p.pop;
+    const R usq = (R)1.5 * (k.u_init[0] * k.u_init[0] + k.u_init[1] * k.u_init[1] + k.u_init[2] * k.u_init[2]);
+#pragma unroll
+    for (int i = 0; i < 19; i++)
+        Pop<S>::st(pop + (size_t)i * p.N + n, feq_i<R>(i, (R)0, (R)1, k.u_init[0], k.u_init[1], k.u_init[2], usq), n * 19u + (uint32_t)i, 0u);
+}
+
+// ---------------------------------------------------------------- dump
+// shader.rs:599-621, 786-792: (rho, u) between steps; NaN off the fluid
+template <class S, int Q>
+__global__ void __launch_bounds__(BLOCK) k_dump(const __grid_constant__ LatParams p) {
+    using R = typename Pop<S>::real;
+    const Consts<R> &k = K<R>(p);
+    const uint32_t n = blockIdx.x * BLOCK + threadIdx.x;
+    if (n >= p.N) return;
+    const uint32_t fg = p.flags[n];
+    if (fg & 3u) { p.dump[n] = make_float4(__int_as_float(0x7fc00000), __int_as_float(0x7fc00000), __int_as_float(0x7fc00000), __int_as_float(0x7fc00000)); return; }
+    const uint32_t rec = fg >> 2;
+    if (rec) {
+        p.dump[n] = make_float4((float)Rec<R>::macro(p, rec - 1, 0), (float)Rec<R>::macro(p, rec - 1, 1), (float)Rec<R>::macro(p, rec - 1, 2),
+                                (float)Rec<R>::macro(p, rec - 1, 3));
+        return;
+    }
+    uint32_t x, y, z;
+    coords(p, n, x, y, z);
+    const Nb nb = make_nb(p, x, y, z);
+    R f[19];
+    load_prev_out<S, Q>(p, n, nb, f);
+    const Moments<R> mo = moments<R>(f);
+    const R rho = (R)1 + mo.rho1;
+    p.dump[n] = make_float4((float)rho, (float)(mo.jx / rho - (R)0.5 * k.grav[0]), (float)(mo.jy / rho - (R)0.5 * k.grav[1]),
+                            (float)(mo.jz / rho - (R)0.5 * k.grav[2]));
+}
+
+// ---------------------------------------------------------------- sampling
+// Density and velocity of a cell between steps (shader.rs:599-621): wall
+// cells from their records, fluid cells from their last post-collision
+// populations, nothing for solid and face cells.
+template <class S, int Q>
+__device__ __forceinline__ bool cell_macro(const LatParams &p, uint32_t m, float &rho, float &ux, float &uy, float &uz) {
+    using R = typename Pop<S>::real;
+    const Consts<R> &k = K<R>(p);
+    const uint32_t fg = p.flags[m];
+    if (fg & 3u) return false;
+    const uint32_t rec = fg >> 2;
+    if (rec) {
+        rho = (float)Rec<R>::macro(p, rec - 1, 0);
+        ux = (float)Rec<R>::macro(p, rec - 1, 1);
+        uy = (float)Rec<R>::macro(p, rec - 1, 2);
+        uz = (float)Rec<R>::macro(p, rec - 1, 3);
+        return true;
+    }
+    uint32_t x, y, z;
+    coords(p, m, x, y, z);
+    const Nb nb = make_nb(p, x, y, z);
+    R f[19];
+    load_prev_out<S, Q>(p, m, nb, f);
+    const Moments<R> mo = moments<R>(f);
+    const R r = (R)1 + mo.rho1;
+    rho = (float)r;
+    ux = (float)(mo.jx / r - (R)0.5 * k.grav[0]);
+    uy = (float)(mo.jy / r - (R)0.5 * k.grav[1]);
+    uz = (float)(mo.jz / r - (R)0.5 * k.grav[2]);
+    return true;
+}
+
+// shader.rs:736-759: trilinear density at rotated surface points
+template <class S, int Q>
+__global__ void __launch_bounds__(BLOCK) k_sample_verts(const __grid_constant__ LatParams p, const __grid_constant__ StepParams s,
+                                                        const float *verts, uint32_t nvert, float voff, double *vacc) {
+    const uint32_t v = blockIdx.x * BLOCK + threadIdx.x;
+    if (v >= nvert) return;
+    const float bx = verts[8 * v] + voff * verts[8 * v + 4];
+    const float by = verts[8 * v + 1] + voff * verts[8 * v + 5];
+    const float bz = verts[8 * v + 2] + voff * verts[8 * v + 6];
+    float sp[3];
+    for (int a = 0; a < 3; a++) sp[a] = p.kf.center[a] + (s.rot[a * 3] * bx + s.rot[a * 3 + 1] * by + s.rot[a * 3 + 2] * bz);
+    const float b0[3] = {floorf(sp[0]), floorf(sp[1]), floorf(sp[2])};
+    const float fr[3] = {sp[0] - b0[0], sp[1] - b0[1], sp[2] - b0[2]};
+    float acc = 0.f, wsum = 0.f;
+    for (int c = 0; c < 8; c++) {
+        const int o[3] = {c & 1, (c >> 1) & 1, (c >> 2) & 1};
+        const int ci[3] = {(int)b0[0] + o[0], (int)b0[1] + o[1], (int)b0[2] + o[2]};
+        if (ci[0] < 1 || ci[1] < 1 || ci[2] < 1 || ci[0] >= (int)p.NX - 1 || ci[1] >= (int)p.NY - 1 || ci[2] >= (int)p.NZ - 1) continue;
+        const float w = (o[0] ? fr[0] : 1.f - fr[0]) * (o[1] ? fr[1] : 1.f - fr[1]) * (o[2] ? fr[2] : 1.f - fr[2]);
+        float rho, ux, uy, uz;
+        const uint32_t m = ((uint32_t)ci[2] * p.NY + (uint32_t)ci[1]) * p.NX + (uint32_t)ci[0];
+        if (cell_macro<S, Q>(p, m, rho, ux, uy, uz) && w > 0.f) { acc += w * rho; wsum += w; }
+    }
+    if (wsum > 1e-6f) {
+        vacc[2 * v] += (double)(acc / wsum);
+        vacc[2 * v + 1] += 1.0;
+    }
+}
+
+// shader.rs:761-784: running sums of (rho, u) at slice pixels
+template <class S, int Q>
+__global__ void __launch_bounds__(BLOCK) k_sample_slices(const __grid_constant__ LatParams p, const int32_t *sd, uint32_t nslices,
+                                                         uint32_t npix, double *sacc) {
+    const uint32_t k = blockIdx.x * BLOCK + threadIdx.x;
+    if (k >= npix) return;
+    uint32_t acc = 0;
+    for (uint32_t sl = 0; sl < nslices; sl++) {
+        const int32_t *o = sd + 4 + 12 * sl;
+        const uint32_t nu = (uint32_t)o[3], nv = (uint32_t)o[7];
+        if (k < acc + nu * nv) {
+            const uint32_t l = k - acc, iv = l / nu, iu = l - iv * nu;
+            const long long c[3] = {(long long)o[0] + (long long)iu * o[4] + (long long)iv * o[8],
+                                    (long long)o[1] + (long long)iu * o[5] + (long long)iv * o[9],
+                                    (long long)o[2] + (long long)iu * o[6] + (long long)iv * o[10]};
+            if (c[0] < 0 || c[1] < 0 || c[2] < 0 || c[0] >= p.NX || c[1] >= p.NY || c[2] >= p.NZ) return;
+            float rho, ux, uy, uz;
+            if (cell_macro<S, Q>(p, ((uint32_t)c[2] * p.NY + (uint32_t)c[1]) * p.NX + (uint32_t)c[0], rho, ux, uy, uz)) {
+                double *b = sacc + 5ull * k;
+                b[0] += rho; b[1] += ux; b[2] += uy; b[3] += uz; b[4] += 1.0;
+            }
+            return;
+        }
+        acc += nu * nv;
+    }
+}
+
+// ---------------------------------------------------------------- mass
+// FP64 sum of rho over fluid cells (wall cells from their records) and a
+// count of non-finite densities.
+template <class S, int Q>
+__global__ void __launch_bounds__(BLOCK) k_mass(const __grid_constant__ LatParams p, double *mass, unsigned long long *bad) {
+    using R = typename Pop<S>::real;
+    const uint32_t n = blockIdx.x * BLOCK + threadIdx.x;
+    double v = 0;
+    unsigned nb_bad = 0;
+    if (n < p.N) {
+        const uint32_t fg = p.flags[n];
+        if ((fg & 3u) == 0u) {
+            const uint32_t rec = fg >> 2;
+            double rho;
+            if (rec) {
+                rho = (double)Rec<R>::macro(p, rec - 1, 0);
+            } else {
+                uint32_t x, y, z;
+                coords(p, n, x, y, z);
+                const Nb nb = make_nb(p, x, y, z);
+                R f[19];
+                load_prev_out<S, Q>(p, n, nb, f);
+                double s = 0;
+#pragma unroll
+                for (int i = 0; i < 19; i++) s += (double)f[i];
+                rho = 1.0 + s;
+            }
+            if (isfinite(rho)) v = rho; else nb_bad = 1;
+        }
+    }
+    v = warp_sum(v);
+    nb_bad = __reduce_add_sync(0xffffffffu, nb_bad);
+    if ((threadIdx.x & 31) == 0) {
+        if (v != 0.0) atomicAdd(mass, v);
+        if (nb_bad) atomicAdd(bad, (unsigned long long)nb_bad);
+    }
+}
+
+// ---------------------------------------------------------------- launchers
+static inline unsigned blocks_for(uint64_t n) { return (unsigned)((n + BLOCK - 1) / BLOCK); }
+
+template <class S, int P, int COLL>
+static cudaError_t step_t(const LatParams &p, const StepParams &s, cudaStream_t st, cudaEvent_t *ev) {
+    if (ev) cudaEventRecord(ev[0], st);
+    if (p.nface) k_faces<S, P><<<blocks_for(p.nface), BLOCK, 0, st>>>(p, s);
+    if (ev) cudaEventRecord(ev[1], st);
+    if (p.nrec) k_walls<S, P, COLL><<<blocks_for(p.nrec), BLOCK, 0, st>>>(p, s);
+    if (ev) cudaEventRecord(ev[2], st);
+    k_bulk<S, P, COLL><<<blocks_for(p.N), BLOCK, 0, st>>>(p, s);
+    if (ev) cudaEventRecord(ev[3], st);
+    return cudaGetLastError();
+}
+
+template <class S>
+static cudaError_t step_s(const LatParams &p, const StepParams &s, int parity, int coll, cudaStream_t st, cudaEvent_t *ev) {
+    if (parity == 0) return coll == 1 ? step_t<S, 0, 1>(p, s, st, ev) : step_t<S, 0, 0>(p, s, st, ev);
+    return coll == 1 ? step_t<S, 1, 1>(p, s, st, ev) : step_t<S, 1, 0>(p, s, st, ev);
+}
+
+cudaError_t launch_step(int storage, const LatParams &p, const StepParams &s, int parity, int coll, cudaStream_t st, cudaEvent_t *ev) {
+    switch (storage) {
+        case 0: return step_s<float>(p, s, parity, coll, st, ev);
+        case 1: return step_s<__half>(p, s, parity, coll, st, ev);
+        case 2: return step_s<__nv_bfloat16>(p, s, parity, coll, st, ev);
+        case 3: return step_s<double>(p, s, parity, coll, st, ev);
+    }
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_init(int storage, const LatParams &p, cudaStream_t st) {
+    const unsigned g = blocks_for(p.N);
+    switch (storage) {
+        case 0: k_init<float><<<g, BLOCK, 0, st>>>(p); break;
+        case 1: k_init<__half><<<g, BLOCK, 0, st>>>(p); break;
+        case 2: k_init<__nv_bfloat16><<<g, BLOCK, 0, st>>>(p); break;
+        case 3: k_init<double><<<g, BLOCK, 0, st>>>(p); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <class S>
+static void dump_s(const LatParams &p, int q, cudaStream_t st) {
+    const unsigned g = blocks_for(p.N);
+    if (q == 0) k_dump<S, 0><<<g, BLOCK, 0, st>>>(p);
+    else k_dump<S, 1><<<g, BLOCK, 0, st>>>(p);
+}
+
+cudaError_t launch_dump(int storage, const LatParams &p, int q, cudaStream_t st) {
+    switch (storage) {
+        case 0: dump_s<float>(p, q, st); break;
+        case 1: dump_s<__half>(p, q, st); break;
+        case 2: dump_s<__nv_bfloat16>(p, q, st); break;
+        case 3: dump_s<double>(p, q, st); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <class S>
+static void mass_s(const LatParams &p, int q, double *mass, unsigned long long *bad, cudaStream_t st) {
+    const unsigned g = blocks_for(p.N);
+    if (q == 0) k_mass<S, 0><<<g, BLOCK, 0, st>>>(p, mass, bad);
+    else k_mass<S, 1><<<g, BLOCK, 0, st>>>(p, mass, bad);
+}
+
+cudaError_t launch_mass(int storage, const LatParams &p, int q, double *mass, unsigned long long *bad, cudaStream_t st) {
+    switch (storage) {
+        case 0: mass_s<float>(p, q, mass, bad, st); break;
+        case 1: mass_s<__half>(p, q, mass, bad, st); break;
+        case 2: mass_s<__nv_bfloat16>(p, q, mass, bad, st); break;
+        case 3: mass_s<double>(p, q, mass, bad, st); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <class S>
+static void sample_s(const LatParams &p, const StepParams &s, int q, const float *verts, uint32_t nvert, float voff, double *vacc,
+                     const int32_t *sd, uint32_t nslices, uint32_t npix, double *sacc, cudaStream_t st) {
+    if (nvert) {
+        if (q == 0) k_sample_verts<S, 0><<<blocks_for(nvert), BLOCK, 0, st>>>(p, s, verts, nvert, voff, vacc);
+        else k_sample_verts<S, 1><<<blocks_for(nvert), BLOCK, 0, st>>>(p, s, verts, nvert, voff, vacc);
+    }
+    if (npix) {
+        if (q == 0) k_sample_slices<S, 0><<<blocks_for(npix), BLOCK, 0, st>>>(p, sd, nslices, npix, sacc);
+        else k_sample_slices<S, 1><<<blocks_for(npix), BLOCK, 0, st>>>(p, sd, nslices, npix, sacc);
+    }
+}
+
+cudaError_t launch_sample(int storage, const LatParams &p, const StepParams &s, int q, const float *verts, uint32_t nvert, float voff,
+                          double *vacc, const int32_t *sd, uint32_t nslices, uint32_t npix, double *sacc, cudaStream_t st) {
+    switch (storage) {
+        case 0: sample_s<float>(p, s, q, verts, nvert, voff, vacc, sd, nslices, npix, sacc, st); break;
+        case 1: sample_s<__half>(p, s, q, verts, nvert, voff, vacc, sd, nslices, npix, sacc, st); break;
+        case 2: sample_s<__nv_bfloat16>(p, s, q, verts, nvert, voff, vacc, sd, nslices, npix, sacc, st); break;
+        case 3: sample_s<double>(p, s, q, verts, nvert, voff, vacc, sd, nslices, npix, sacc, st); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace lbm

@@ -1,0 +1,695 @@
+// Host driver of the D3Q19 engine and the C ABI of include/simlab_lbm.h.
+//
+// Mirrors `Lattice` of crates/cfd/src/lattice.rs: setup validation (233-271),
+// face list (283-324), wall records (454-482, record_words 202-218), flags
+// (489-526), initial state (661-671), the per-step dispatch (701-753), field
+// and record readback (785-841).  Differences by design: one allocation per
+// buffer in HBM (no 4 GiB split), one CUDA stream per handle, device waits
+// bounded by a host-side limit, forces summed in FP64.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/simlab_lbm.h"
+#include "lbm_kernels.h"
+#include "voxel.hpp"
+
+namespace {
+
+thread_local std::string g_error;
+
+constexpr uint32_t KMAX = 512;  // steps per readback chunk (lattice.rs:134)
+
+struct LbmError : std::runtime_error {
+    int code;
+    LbmError(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+inline void ck(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) {
+        int code = (e == cudaErrorMemoryAllocation) ? LBM_ERR_NOMEM : LBM_ERR_CUDA;
+        throw LbmError(code, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+
+inline uint32_t fbits(float x) { uint32_t b; std::memcpy(&b, &x, 4); return b; }
+
+// lattice.rs:172-189
+uint16_t f16_bits(float x) {
+    uint32_t b = fbits(x);
+    uint16_t sign = (uint16_t)((b >> 16) & 0x8000u);
+    int exp = (int)((b >> 23) & 0xffu) - 127 + 15;
+    uint32_t man = b & 0x7fffffu;
+    if (exp <= 0) return sign;
+    if (exp >= 31) return (uint16_t)(sign | 0x7c00u);
+    uint32_t h = (uint32_t)sign | ((uint32_t)exp << 10) | (man >> 13);
+    if (man & 0x1000u) h += 1;
+    return (uint16_t)h;
+}
+
+inline double weight19(int i) { return i == 0 ? 1.0 / 3.0 : (i <= 6 ? 1.0 / 18.0 : 1.0 / 36.0); }
+
+size_t storage_bytes(int s) { return s == LBM_STORAGE_FP32 ? 4 : (s == LBM_STORAGE_FP64 ? 8 : 2); }
+
+}  // namespace
+
+struct lbm_lattice {
+    lbm_setup setup{};
+    lbm::LatParams lp{};
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    std::vector<void *> allocs;
+    uint64_t steps_done = 0;
+    uint64_t memory_bytes = 0;
+    uint32_t nrec = 0, nface = 0, npix = 0, nvert = 0;
+    double timeout_s = 600.0;
+    std::string err;
+    // sampling
+    double *vacc = nullptr;     // 2 doubles per vertex (sum, count)
+    double *sacc = nullptr;     // 5 doubles per pixel
+    float *verts = nullptr;     // 8 floats per vertex
+    int32_t *slicedef = nullptr;
+    uint32_t nslices = 0;
+    float voff = 0.f;
+    double *hist_host = nullptr;  // pinned
+    cudaEvent_t ev = nullptr;
+    // kernel profiling: 4 events per profiled step
+    bool prof = false;
+    std::vector<cudaEvent_t> prof_ev;
+    uint64_t prof_steps = 0;
+
+    void *dalloc(size_t bytes) {
+        void *p = nullptr;
+        ck(cudaMalloc(&p, std::max<size_t>(bytes, 16)), "cudaMalloc");
+        allocs.push_back(p);
+        memory_bytes += std::max<size_t>(bytes, 16);
+        return p;
+    }
+    ~lbm_lattice() {
+        if (stream) cudaStreamSynchronize(stream);
+        for (void *p : allocs) cudaFree(p);
+        if (hist_host) cudaFreeHost(hist_host);
+        if (ev) cudaEventDestroy(ev);
+        for (cudaEvent_t e : prof_ev) cudaEventDestroy(e);
+        if (stream) cudaStreamDestroy(stream);
+    }
+    void wait() {
+        ck(cudaEventRecord(ev, stream), "cudaEventRecord");
+        auto t0 = std::chrono::steady_clock::now();
+        for (;;) {
+            cudaError_t q = cudaEventQuery(ev);
+            if (q == cudaSuccess) return;
+            if (q != cudaErrorNotReady) ck(q, "device wait");
+            double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            if (el > timeout_s) throw LbmError(LBM_ERR_TIMEOUT, "device did not finish within " + std::to_string(timeout_s) + " s");
+            if (el > 1e-3) std::this_thread::sleep_for(std::chrono::microseconds(50));
+        }
+    }
+    int parity() const { return (int)(steps_done % 2); }
+};
+
+namespace {
+
+int fail(lbm_lattice *h, const LbmError &e) {
+    if (h) h->err = e.what(); else g_error = e.what();
+    return e.code;
+}
+
+template <class F>
+int guard(lbm_lattice *h, F &&fn) {
+    try {
+        fn();
+        return LBM_OK;
+    } catch (const LbmError &e) {
+        return fail(h, e);
+    } catch (const std::exception &e) {
+        return fail(h, LbmError(LBM_ERR_INVALID, e.what()));
+    }
+}
+
+template <class R>
+void fill_consts(lbm::Consts<R> &k, const lbm_setup &st) {
+    k.tau0 = (R)(0.5 + 3.0 * st.nu);
+    k.smag2 = (R)(st.smagorinsky * st.smagorinsky);
+    k.sponge_tau = (R)st.sponge_tau;
+    k.sigma = (R)st.sponge_sigma;
+    for (int a = 0; a < 3; a++) {
+        k.sp_lo[a] = (R)st.sponge[2 * a];
+        k.sp_hi[a] = (R)st.sponge[2 * a + 1];
+        k.u_inf[a] = (R)st.u_inf[a];
+        k.u_init[a] = (R)st.u_init[a];
+        k.grav[a] = (R)st.body_force[a];
+        k.center[a] = (R)st.center[a];
+    }
+}
+
+lbm::StepParams step_params(const lbm_lattice *h, const lbm_step_in &s, uint32_t slot, uint64_t step_index) {
+    lbm::StepParams sp{};
+    sp.seed = (uint32_t)step_index * 2654435761u;  // lattice.rs:676
+    sp.slot = slot;
+    for (int a = 0; a < 3; a++) {
+        sp.omega[a] = (float)s.omega[a];
+        sp.omega_d[a] = s.omega[a];
+    }
+    for (int r = 0; r < 3; r++)
+        for (int c = 0; c < 3; c++) sp.rot[r * 3 + c] = (float)s.rot[r][c];
+    (void)h;
+    return sp;
+}
+
+void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_probes *probes, lbm_lattice *h) {
+    if (!setup) throw LbmError(LBM_ERR_INVALID, "setup is null");
+    const lbm_setup &st = *setup;
+    const uint64_t NX = st.dims[0], NY = st.dims[1], NZ = st.dims[2];
+    const uint64_t N = NX * NY * NZ;
+    // lattice.rs:233-244
+    if (N == 0 || N >= 0xffffffffull) throw LbmError(LBM_ERR_INVALID, "grid of " + std::to_string(N) + " cells is out of range");
+    if (NX < 3 || NY < 3 || NZ < 3) throw LbmError(LBM_ERR_INVALID, "grid must be at least 3 cells in every direction");
+    int per[3];
+    for (int a = 0; a < 3; a++) {
+        bool p0 = st.faces[2 * a] == LBM_FACE_PERIODIC, p1 = st.faces[2 * a + 1] == LBM_FACE_PERIODIC;
+        if (p0 != p1) throw LbmError(LBM_ERR_INVALID, "periodic faces must come in pairs");
+        per[a] = p0;
+    }
+    for (int f = 0; f < 6; f++)
+        if (st.faces[f] < LBM_FACE_VELOCITY || st.faces[f] > LBM_FACE_FREE_SLIP) throw LbmError(LBM_ERR_INVALID, "unknown face type");
+    if (st.storage < LBM_STORAGE_FP32 || st.storage > LBM_STORAGE_FP64) throw LbmError(LBM_ERR_INVALID, "unknown storage");
+    if (st.collision != LBM_COLLISION_REGULARIZED && st.collision != LBM_COLLISION_BGK) throw LbmError(LBM_ERR_INVALID, "unknown collision");
+    if (!(st.nu > 0.0) || !std::isfinite(st.nu)) throw LbmError(LBM_ERR_INVALID, "viscosity must be positive");
+    if (geom && geom->kind != 0 && geom->kind != 1)
+        throw LbmError(LBM_ERR_UNSUPPORTED, "only static geometry is supported by this lattice");
+    h->setup = st;
+
+    // face cells (lattice.rs:283-324) plus free slip: velocity sticks,
+    // otherwise the later face in -x,+x,-y,+y,-z,+z order wins; free-slip
+    // faces collect their mirror axes.
+    std::vector<uint32_t> faces;
+    std::vector<uint8_t> finfo;
+    auto face_type = [&](uint64_t x, uint64_t y, uint64_t z, uint8_t &info) -> bool {
+        bool on[6] = {x == 0, x == NX - 1, y == 0, y == NY - 1, z == 0, z == NZ - 1};
+        int ty = -1;
+        uint8_t mir = 0;
+        for (int f = 0; f < 6; f++) {
+            if (on[f] && st.faces[f] != LBM_FACE_PERIODIC) {
+                int t = st.faces[f] == LBM_FACE_VELOCITY ? 0 : (st.faces[f] == LBM_FACE_OPEN ? 1 : 2);
+                if (st.faces[f] == LBM_FACE_FREE_SLIP) mir |= (uint8_t)(1u << (f / 2));
+                ty = (ty == 0) ? 0 : t;
+            }
+        }
+        if (ty < 0) return false;
+        info = (uint8_t)(ty | (ty == 2 ? (mir << 2) : 0));
+        return true;
+    };
+    for (uint64_t z = 0; z < NZ; z++)
+        for (uint64_t y = 0; y < NY; y++) {
+            bool edge = y == 0 || y == NY - 1 || z == 0 || z == NZ - 1;
+            auto visit = [&](uint64_t x) {
+                uint8_t info;
+                if (face_type(x, y, z, info)) { faces.push_back((uint32_t)((z * NY + y) * NX + x)); finfo.push_back(info); }
+            };
+            if (edge) { for (uint64_t x = 0; x < NX; x++) visit(x); }
+            else { visit(0); visit(NX - 1); }
+        }
+    h->nface = (uint32_t)faces.size();
+
+    // wall records (lattice.rs:454-482; record_words 202-218)
+    const bool stat = geom && geom->kind == 1;
+    const uint64_t nrec = stat ? geom->nwalls : 0;
+    if (nrec >= 0x3fffffffull) throw LbmError(LBM_ERR_INVALID, "too many wall records");
+    h->nrec = (uint32_t)nrec;
+    std::vector<uint32_t> words(nrec * lbm::RS, 0);
+    std::vector<double> wordsd;
+    if (st.storage == LBM_STORAGE_FP64) wordsd.assign(nrec * lbm::RD, 0.0);
+    {
+        float fe[19];
+        double fed[19];
+        double usq = 1.5 * (st.u_init[0] * st.u_init[0] + st.u_init[1] * st.u_init[1] + st.u_init[2] * st.u_init[2]);
+        for (int i = 0; i < 19; i++) {
+            double cu = lbm::CX(i) * st.u_init[0] + lbm::CY(i) * st.u_init[1] + lbm::CZ(i) * st.u_init[2];
+            fed[i] = weight19(i) * (3.0 * cu + 4.5 * cu * cu - usq);
+            fe[i] = (float)fed[i];
+        }
+        for (uint64_t r = 0; r < nrec; r++) {
+            const lbm_wall_cell &w = geom->walls[r];
+            if (w.cell >= N) throw LbmError(LBM_ERR_INVALID, "wall cell index outside the grid");
+            uint32_t *o = words.data() + r * lbm::RS;
+            o[lbm::R_MASK] = w.mask & 0x7fffeu;  // directions 1..18
+            o[lbm::R_CELL] = w.cell;
+            for (int k = 0; k < 9; k++) o[lbm::R_Q + k] = (uint32_t)f16_bits(w.q[2 * k + 1]) | ((uint32_t)f16_bits(w.q[2 * k + 2]) << 16);
+            for (int i = 1; i < 19; i++) o[lbm::R_FPOST + i - 1] = fbits(fe[i]);
+            o[lbm::R_MACRO] = fbits(1.0f);
+            for (int a = 0; a < 3; a++) o[lbm::R_MACRO + 1 + a] = fbits((float)st.u_init[a]);
+            if (!wordsd.empty()) {
+                double *d = wordsd.data() + r * lbm::RD;
+                for (int i = 1; i < 19; i++) d[lbm::RD_FPOST + i - 1] = fed[i];
+                d[lbm::RD_MACRO] = 1.0;
+                for (int a = 0; a < 3; a++) d[lbm::RD_MACRO + 1 + a] = st.u_init[a];
+            }
+        }
+    }
+    // flags (lattice.rs:489-526)
+    std::vector<uint32_t> flags(N, 0);
+    for (size_t k = 0; k < faces.size(); k++) flags[faces[k]] = (finfo[k] & 3u) == 0 ? 2u : 3u;
+    if (stat) {
+        for (uint64_t s = 0; s < geom->nsolid; s++) {
+            uint32_t c = geom->solid[s];
+            if (c >= N) throw LbmError(LBM_ERR_INVALID, "solid cell index outside the grid");
+            if (flags[c] == 0) flags[c] = 1;
+        }
+        for (uint64_t r = 0; r < nrec; r++) {
+            uint32_t c = geom->walls[r].cell;
+            if ((flags[c] & 3u) == 0) flags[c] = (uint32_t)(r + 1) << 2;  // a later record of the same cell wins
+        }
+    }
+
+    // probes
+    std::vector<float> vbuf;
+    std::vector<int32_t> sd(4, 0);
+    if (probes) {
+        h->nvert = (uint32_t)probes->nvert;
+        for (uint64_t v = 0; v < probes->nvert; v++) {
+            const double *q = probes->verts + 6 * v;
+            float e[8] = {(float)q[0], (float)q[1], (float)q[2], 0.f, (float)q[3], (float)q[4], (float)q[5], 0.f};
+            vbuf.insert(vbuf.end(), e, e + 8);
+        }
+        h->nslices = (uint32_t)probes->nslices;
+        sd[0] = (int32_t)probes->nslices;
+        uint64_t npix = 0;
+        for (uint64_t s = 0; s < probes->nslices; s++) {
+            const lbm_slice_def &d = probes->slices[s];
+            int32_t e[12] = {d.origin[0], d.origin[1], d.origin[2], (int32_t)d.nu, d.u[0], d.u[1], d.u[2], (int32_t)d.nv, d.v[0], d.v[1], d.v[2], 0};
+            sd.insert(sd.end(), e, e + 12);
+            npix += (uint64_t)d.nu * d.nv;
+        }
+        if (npix >= 0xffffffffull) throw LbmError(LBM_ERR_INVALID, "too many slice pixels");
+        h->npix = (uint32_t)npix;
+        h->voff = (float)probes->vertex_offset;
+    }
+
+    // device buffers
+    ck(cudaGetDevice(&h->device), "cudaGetDevice");
+    ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    ck(cudaEventCreateWithFlags(&h->ev, cudaEventDisableTiming), "cudaEventCreate");
+    ck(cudaMallocHost((void **)&h->hist_host, KMAX * 8 * sizeof(double)), "cudaMallocHost");
+    lbm::LatParams &p = h->lp;
+    const size_t sb = storage_bytes(st.storage);
+    p.pop = h->dalloc(19 * N * sb);
+    p.flags = (uint32_t *)h->dalloc(N * 4);
+    p.recs = (uint32_t *)h->dalloc(nrec * lbm::RS * 4);
+    p.recd = st.storage == LBM_STORAGE_FP64 ? (double *)h->dalloc(nrec * lbm::RD * 8) : nullptr;
+    p.faces = (uint32_t *)h->dalloc(faces.size() * 4);
+    p.face_info = (uint8_t *)h->dalloc(finfo.size());
+    const uint64_t nwb = (nrec + lbm::BLOCK - 1) / lbm::BLOCK;
+    p.partials = (double *)h->dalloc(std::max<uint64_t>(nwb, 1) * 8 * sizeof(double));
+    p.ticket = (uint32_t *)h->dalloc(16);
+    p.hist = (double *)h->dalloc(KMAX * 8 * sizeof(double));
+    p.dump = st.debug_dump ? (float4 *)h->dalloc(N * 16) : nullptr;
+    h->vacc = (double *)h->dalloc(std::max<uint64_t>(h->nvert, 1) * 2 * sizeof(double));
+    h->sacc = (double *)h->dalloc(std::max<uint64_t>(h->npix, 1) * 5 * sizeof(double));
+    h->verts = (float *)h->dalloc(std::max<size_t>(vbuf.size(), 8) * 4);
+    h->slicedef = (int32_t *)h->dalloc(sd.size() * 4);
+    p.NX = (uint32_t)NX; p.NY = (uint32_t)NY; p.NZ = (uint32_t)NZ; p.N = (uint32_t)N;
+    p.nrec = (uint32_t)nrec; p.nface = (uint32_t)faces.size();
+    for (int a = 0; a < 3; a++) p.per[a] = per[a];
+    p.abs_u = st.absorb_velocity != 0;
+    p.total_p = st.total_pressure_inlet != 0;
+    p.wall_model = st.wall_model != 0;
+    p.forcing = st.body_force[0] != 0.0 || st.body_force[1] != 0.0 || st.body_force[2] != 0.0;
+    p.sponge_on = 0;
+    for (int f = 0; f < 6; f++) p.sponge_on |= st.sponge[f] > 0;
+    p.les_on = st.smagorinsky != 0.0;
+    p.moving = 0;
+    fill_consts<float>(p.kf, st);
+    fill_consts<double>(p.kd, st);
+
+    cudaStream_t s = h->stream;
+    ck(cudaMemcpyAsync(p.flags, flags.data(), N * 4, cudaMemcpyHostToDevice, s), "upload flags");
+    if (nrec) ck(cudaMemcpyAsync(p.recs, words.data(), words.size() * 4, cudaMemcpyHostToDevice, s), "upload records");
+    if (!wordsd.empty()) ck(cudaMemcpyAsync(p.recd, wordsd.data(), wordsd.size() * 8, cudaMemcpyHostToDevice, s), "upload records");
+    if (!faces.empty()) {
+        ck(cudaMemcpyAsync((void *)p.faces, faces.data(), faces.size() * 4, cudaMemcpyHostToDevice, s), "upload faces");
+        ck(cudaMemcpyAsync((void *)p.face_info, finfo.data(), finfo.size(), cudaMemcpyHostToDevice, s), "upload faces");
+    }
+    if (!vbuf.empty()) ck(cudaMemcpyAsync(h->verts, vbuf.data(), vbuf.size() * 4, cudaMemcpyHostToDevice, s), "upload vertices");
+    ck(cudaMemcpyAsync(h->slicedef, sd.data(), sd.size() * 4, cudaMemcpyHostToDevice, s), "upload slices");
+    ck(cudaMemsetAsync(p.ticket, 0, 16, s), "memset");
+    ck(cudaMemsetAsync(p.hist, 0, KMAX * 8 * sizeof(double), s), "memset");
+    ck(cudaMemsetAsync(h->vacc, 0, std::max<uint64_t>(h->nvert, 1) * 2 * sizeof(double), s), "memset");
+    ck(cudaMemsetAsync(h->sacc, 0, std::max<uint64_t>(h->npix, 1) * 5 * sizeof(double), s), "memset");
+    ck(lbm::launch_init(st.storage, p, s), "init kernel");
+    h->wait();  // host vectors go out of scope after this
+}
+
+void run_impl(lbm_lattice *h, const lbm_step_in *steps, uint64_t n, double *forces_out, bool readback) {
+    if (n && !steps) throw LbmError(LBM_ERR_INVALID, "steps is null");
+    lbm::LatParams &p = h->lp;
+    lbm_step_in still{};
+    for (int a = 0; a < 3; a++) { still.rot[a][a] = 1.0; still.rot_prev[a][a] = 1.0; }
+    for (uint64_t c0 = 0; c0 < n; c0 += KMAX) {
+        const uint32_t len = (uint32_t)std::min<uint64_t>(KMAX, n - c0);
+        if (p.nrec == 0) ck(cudaMemsetAsync(p.hist, 0, len * 8 * sizeof(double), h->stream), "memset");
+        for (uint32_t k = 0; k < len; k++) {
+            const lbm_step_in &si = steps ? steps[c0 + k] : still;
+            const uint64_t idx = h->steps_done;
+            lbm::StepParams sp = step_params(h, si, k, idx);
+            cudaEvent_t *evs = nullptr;
+            if (h->prof) {
+                const size_t need = 4 * (h->prof_steps + 1);
+                while (h->prof_ev.size() < need) {
+                    cudaEvent_t e;
+                    ck(cudaEventCreate(&e), "cudaEventCreate");
+                    h->prof_ev.push_back(e);
+                }
+                evs = h->prof_ev.data() + 4 * h->prof_steps;
+                h->prof_steps++;
+            }
+            ck(lbm::launch_step(h->setup.storage, p, sp, (int)(idx % 2), h->setup.collision, h->stream, evs), "step kernels");
+            if (si.sample && (h->nvert || h->npix))
+                ck(lbm::launch_sample(h->setup.storage, p, sp, (int)(idx % 2), h->verts, h->nvert, h->voff, h->vacc, h->slicedef,
+                                      h->nslices, h->npix, h->sacc, h->stream),
+                   "sample kernels");
+            h->steps_done++;
+        }
+        if (readback) {
+            ck(cudaMemcpyAsync(h->hist_host, p.hist, len * 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "history readback");
+            h->wait();
+            if (forces_out)
+                for (uint32_t k = 0; k < len; k++)
+                    for (int j = 0; j < 6; j++) forces_out[(c0 + k) * 6 + j] = h->hist_host[k * 8 + j];
+        }
+    }
+}
+
+}  // namespace
+
+// ============================================================== C ABI
+extern "C" {
+
+const char *lbm_version(void) { return "simlab-lbm-b200 0.1 (sm_100a)"; }
+
+int lbm_global_error(char *buf, uint64_t len) {
+    if (buf && len) std::snprintf(buf, (size_t)len, "%s", g_error.c_str());
+    return LBM_OK;
+}
+
+int lbm_last_error(const lbm_lattice *h, char *buf, uint64_t len) {
+    if (!h) return lbm_global_error(buf, len);
+    if (buf && len) std::snprintf(buf, (size_t)len, "%s", h->err.c_str());
+    return LBM_OK;
+}
+
+uint64_t lbm_max_cells(int32_t storage) {
+    (void)storage;
+    return 0xfffffffeull;  // cell indices are 32-bit, as in the reference
+}
+
+int lbm_create(const lbm_setup *setup, const lbm_geometry *geom, const lbm_probes *probes, lbm_lattice **out) {
+    if (!out) { g_error = "out is null"; return LBM_ERR_INVALID; }
+    *out = nullptr;
+    lbm_lattice *h = new lbm_lattice();
+    try {
+        create_impl(setup, geom, probes, h);
+    } catch (const LbmError &e) {
+        g_error = e.what();
+        delete h;
+        return e.code;
+    } catch (const std::exception &e) {
+        g_error = e.what();
+        delete h;
+        return LBM_ERR_INVALID;
+    }
+    *out = h;
+    return LBM_OK;
+}
+
+void lbm_destroy(lbm_lattice *h) { delete h; }
+
+int lbm_run(lbm_lattice *h, const lbm_step_in *steps, uint64_t n, double *forces_out) {
+    if (!h) return LBM_ERR_INVALID;
+    return guard(h, [&] { run_impl(h, steps, n, forces_out, true); });
+}
+
+int lbm_advance(lbm_lattice *h, uint64_t n) {
+    if (!h) return LBM_ERR_INVALID;
+    return guard(h, [&] { run_impl(h, nullptr, n, nullptr, false); });
+}
+
+int lbm_stream(lbm_lattice *h, void **stream) {
+    if (!h || !stream) return LBM_ERR_INVALID;
+    *stream = (void *)h->stream;
+    return LBM_OK;
+}
+
+int lbm_synchronize(lbm_lattice *h) {
+    if (!h) return LBM_ERR_INVALID;
+    return guard(h, [&] { h->wait(); });
+}
+
+int lbm_profile(lbm_lattice *h, int32_t enable) {
+    if (!h) return LBM_ERR_INVALID;
+    return guard(h, [&] {
+        h->wait();
+        h->prof = enable != 0;
+        h->prof_steps = 0;
+    });
+}
+
+int lbm_get_kernel_times(lbm_lattice *h, lbm_kernel_times *out) {
+    if (!h || !out) return LBM_ERR_INVALID;
+    return guard(h, [&] {
+        h->wait();
+        out->steps = h->prof_steps;
+        out->faces_ms = out->walls_ms = out->bulk_ms = 0.0;
+        for (uint64_t k = 0; k < h->prof_steps; k++) {
+            cudaEvent_t *e = h->prof_ev.data() + 4 * k;
+            float a, b, c;
+            ck(cudaEventElapsedTime(&a, e[0], e[1]), "cudaEventElapsedTime");
+            ck(cudaEventElapsedTime(&b, e[1], e[2]), "cudaEventElapsedTime");
+            ck(cudaEventElapsedTime(&c, e[2], e[3]), "cudaEventElapsedTime");
+            out->faces_ms += a;
+            out->walls_ms += b;
+            out->bulk_ms += c;
+        }
+    });
+}
+
+int lbm_set_timeout(lbm_lattice *h, double seconds) {
+    if (!h || !(seconds > 0)) return LBM_ERR_INVALID;
+    h->timeout_s = seconds;
+    return LBM_OK;
+}
+
+int lbm_macros(lbm_lattice *h, float *out) {
+    if (!h || !out) return LBM_ERR_INVALID;
+    return guard(h, [&] {
+        if (!h->setup.debug_dump) throw LbmError(LBM_ERR_STATE, "macros() needs debug_dump");
+        const int q = 1 - h->parity();
+        ck(lbm::launch_dump(h->setup.storage, h->lp, q, h->stream), "dump kernel");
+        ck(cudaMemcpyAsync(out, h->lp.dump, (size_t)h->lp.N * 16, cudaMemcpyDeviceToHost, h->stream), "dump readback");
+        h->wait();
+    });
+}
+
+int lbm_records(lbm_lattice *h, uint32_t *out, uint64_t cap_words) {
+    if (!h || (!out && cap_words)) return LBM_ERR_INVALID;
+    return guard(h, [&] {
+        uint64_t words = (uint64_t)h->nrec * lbm::RS;
+        if (cap_words < words) throw LbmError(LBM_ERR_INVALID, "record buffer too small");
+        if (words) ck(cudaMemcpyAsync(out, h->lp.recs, words * 4, cudaMemcpyDeviceToHost, h->stream), "record readback");
+        h->wait();
+    });
+}
+
+int lbm_reset_samples(lbm_lattice *h) {
+    if (!h) return LBM_ERR_INVALID;
+    return guard(h, [&] {
+        ck(cudaMemsetAsync(h->vacc, 0, std::max<uint64_t>(h->nvert, 1) * 2 * sizeof(double), h->stream), "memset");
+        ck(cudaMemsetAsync(h->sacc, 0, std::max<uint64_t>(h->npix, 1) * 5 * sizeof(double), h->stream), "memset");
+        h->wait();
+    });
+}
+
+int lbm_vertex_means(lbm_lattice *h, float *out) {
+    if (!h || (!out && h->nvert)) return LBM_ERR_INVALID;
+    return guard(h, [&] {
+        if (!h->nvert) return;
+        std::vector<double> v(2 * (size_t)h->nvert);
+        ck(cudaMemcpyAsync(v.data(), h->vacc, v.size() * 8, cudaMemcpyDeviceToHost, h->stream), "vertex readback");
+        h->wait();
+        for (uint32_t i = 0; i < h->nvert; i++) out[i] = v[2 * i + 1] > 0 ? (float)(v[2 * i] / v[2 * i + 1]) : NAN;
+    });
+}
+
+int lbm_slice_means(lbm_lattice *h, float *out) {
+    if (!h || (!out && h->npix)) return LBM_ERR_INVALID;
+    return guard(h, [&] {
+        if (!h->npix) return;
+        std::vector<double> v(5 * (size_t)h->npix);
+        ck(cudaMemcpyAsync(v.data(), h->sacc, v.size() * 8, cudaMemcpyDeviceToHost, h->stream), "slice readback");
+        h->wait();
+        for (uint32_t i = 0; i < h->npix; i++) {
+            double c = v[5 * i + 4];
+            for (int a = 0; a < 4; a++) out[4 * i + a] = c > 0 ? (float)(v[5 * i + a] / c) : NAN;
+        }
+    });
+}
+
+int lbm_get_info(const lbm_lattice *h, lbm_info *out) {
+    if (!h || !out) return LBM_ERR_INVALID;
+    out->steps_done = h->steps_done;
+    out->nrec = h->nrec;
+    out->nface = h->nface;
+    out->npix = h->npix;
+    out->nvert = h->nvert;
+    out->memory_bytes = h->memory_bytes;
+    out->cells = h->lp.N;
+    out->storage = h->setup.storage;
+    out->collision = h->setup.collision;
+    return LBM_OK;
+}
+
+int lbm_mass(lbm_lattice *h, double *mass, uint64_t *nonfinite) {
+    if (!h) return LBM_ERR_INVALID;
+    return guard(h, [&] {
+        double *dm = nullptr;
+        ck(cudaMallocAsync((void **)&dm, 16, h->stream), "cudaMallocAsync");
+        ck(cudaMemsetAsync(dm, 0, 16, h->stream), "memset");
+        ck(lbm::launch_mass(h->setup.storage, h->lp, 1 - h->parity(), dm, (unsigned long long *)(dm + 1), h->stream), "mass kernel");
+        double hv[2];
+        ck(cudaMemcpyAsync(hv, dm, 16, cudaMemcpyDeviceToHost, h->stream), "mass readback");
+        ck(cudaFreeAsync(dm, h->stream), "cudaFreeAsync");
+        h->wait();
+        if (mass) *mass = hv[0];
+        uint64_t bad;
+        std::memcpy(&bad, &hv[1], 8);
+        if (nonfinite) *nonfinite = bad;
+    });
+}
+
+// checkpoint blob: header, populations, records (u32), records (f64, FP64 only)
+struct StateHeader { uint64_t magic, cells, steps_done, nrec; int32_t storage, collision; };
+static const uint64_t STATE_MAGIC = 0x4c424d5354415431ull;
+
+int lbm_state_size(const lbm_lattice *h, uint64_t *bytes) {
+    if (!h || !bytes) return LBM_ERR_INVALID;
+    const uint64_t N = h->lp.N;
+    *bytes = sizeof(StateHeader) + 19 * N * storage_bytes(h->setup.storage) + (uint64_t)h->nrec * lbm::RS * 4 +
+             (h->lp.recd ? (uint64_t)h->nrec * lbm::RD * 8 : 0);
+    return LBM_OK;
+}
+
+int lbm_save_state(lbm_lattice *h, void *buf, uint64_t bytes) {
+    if (!h || !buf) return LBM_ERR_INVALID;
+    return guard(h, [&] {
+        uint64_t need;
+        lbm_state_size(h, &need);
+        if (bytes < need) throw LbmError(LBM_ERR_INVALID, "state buffer too small");
+        StateHeader hd{STATE_MAGIC, h->lp.N, h->steps_done, h->nrec, h->setup.storage, h->setup.collision};
+        char *o = (char *)buf;
+        std::memcpy(o, &hd, sizeof hd);
+        o += sizeof hd;
+        const uint64_t pb = 19ull * h->lp.N * storage_bytes(h->setup.storage);
+        ck(cudaMemcpyAsync(o, h->lp.pop, pb, cudaMemcpyDeviceToHost, h->stream), "state readback");
+        o += pb;
+        if (h->nrec) ck(cudaMemcpyAsync(o, h->lp.recs, (size_t)h->nrec * lbm::RS * 4, cudaMemcpyDeviceToHost, h->stream), "state readback");
+        o += (size_t)h->nrec * lbm::RS * 4;
+        if (h->lp.recd && h->nrec) ck(cudaMemcpyAsync(o, h->lp.recd, (size_t)h->nrec * lbm::RD * 8, cudaMemcpyDeviceToHost, h->stream), "state readback");
+        h->wait();
+    });
+}
+
+int lbm_load_state(lbm_lattice *h, const void *buf, uint64_t bytes) {
+    if (!h || !buf) return LBM_ERR_INVALID;
+    return guard(h, [&] {
+        uint64_t need;
+        lbm_state_size(h, &need);
+        if (bytes < need) throw LbmError(LBM_ERR_INVALID, "state buffer too small");
+        StateHeader hd;
+        std::memcpy(&hd, buf, sizeof hd);
+        if (hd.magic != STATE_MAGIC || hd.cells != h->lp.N || hd.nrec != h->nrec || hd.storage != h->setup.storage)
+            throw LbmError(LBM_ERR_INVALID, "state does not belong to this lattice");
+        const char *o = (const char *)buf + sizeof hd;
+        const uint64_t pb = 19ull * h->lp.N * storage_bytes(h->setup.storage);
+        ck(cudaMemcpyAsync(h->lp.pop, o, pb, cudaMemcpyHostToDevice, h->stream), "state upload");
+        o += pb;
+        if (h->nrec) ck(cudaMemcpyAsync(h->lp.recs, o, (size_t)h->nrec * lbm::RS * 4, cudaMemcpyHostToDevice, h->stream), "state upload");
+        o += (size_t)h->nrec * lbm::RS * 4;
+        if (h->lp.recd && h->nrec) ck(cudaMemcpyAsync(h->lp.recd, o, (size_t)h->nrec * lbm::RD * 8, cudaMemcpyHostToDevice, h->stream), "state upload");
+        h->wait();
+        h->steps_done = hd.steps_done;
+    });
+}
+
+// ------------------------------------------------------------ voxelizer
+struct lbm_voxels {
+    lbm::StaticVoxels v;
+};
+
+static lbm::Surface make_surface(const double *verts, uint64_t nverts, const uint32_t *tris, uint64_t ntris) {
+    lbm::Surface s;
+    s.verts.resize(nverts);
+    for (uint64_t i = 0; i < nverts; i++) s.verts[i] = {verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]};
+    s.tris.resize(ntris);
+    for (uint64_t t = 0; t < ntris; t++) {
+        for (int k = 0; k < 3; k++)
+            if (tris[3 * t + k] >= nverts) throw LbmError(LBM_ERR_INVALID, "triangle vertex index out of range");
+        s.tris[t] = {tris[3 * t], tris[3 * t + 1], tris[3 * t + 2]};
+    }
+    return s;
+}
+
+int lbm_voxelize_static(const double *verts, uint64_t nverts, const uint32_t *tris, uint64_t ntris, const uint32_t dims[3],
+                        int32_t lattice, lbm_voxels **out) {
+    if (!out || !dims || (nverts && !verts) || (ntris && !tris)) { g_error = "null argument"; return LBM_ERR_INVALID; }
+    *out = nullptr;
+    return guard(nullptr, [&] {
+        if (lattice != 19 && lattice != 27) throw LbmError(LBM_ERR_INVALID, "lattice must be 19 or 27");
+        lbm::Surface s = make_surface(verts, nverts, tris, ntris);
+        lbm_voxels *v = new lbm_voxels();
+        v->v = lbm::voxelize_static(s, {dims[0], dims[1], dims[2]}, lattice);
+        *out = v;
+    });
+}
+
+int lbm_voxels_counts(const lbm_voxels *v, uint64_t *nsolid, uint64_t *nwalls) {
+    if (!v) return LBM_ERR_INVALID;
+    if (nsolid) *nsolid = v->v.solid.size();
+    if (nwalls) *nwalls = v->v.walls.size();
+    return LBM_OK;
+}
+
+int lbm_voxels_copy(const lbm_voxels *v, uint32_t *solid, lbm_wall_cell *walls) {
+    if (!v) return LBM_ERR_INVALID;
+    if (solid && !v->v.solid.empty()) std::memcpy(solid, v->v.solid.data(), v->v.solid.size() * 4);
+    if (walls)
+        for (size_t r = 0; r < v->v.walls.size(); r++) {
+            walls[r].cell = v->v.walls[r].cell;
+            walls[r].mask = v->v.walls[r].mask;
+            for (int k = 0; k < 27; k++) walls[r].q[k] = v->v.walls[r].q[k];
+        }
+    return LBM_OK;
+}
+
+void lbm_voxels_free(lbm_voxels *v) { delete v; }
+
+int lbm_inside_grid(const double *verts, uint64_t nverts, const uint32_t *tris, uint64_t ntris, const double origin[3], double h,
+                    const uint32_t dims[3], uint8_t *out) {
+    if (!origin || !dims || !out || (nverts && !verts) || (ntris && !tris)) { g_error = "null argument"; return LBM_ERR_INVALID; }
+    return guard(nullptr, [&] {
+        lbm::Surface s = make_surface(verts, nverts, tris, ntris);
+        lbm::GridSpec g;
+        g.origin = {origin[0], origin[1], origin[2]};
+        g.h = h;
+        g.dims = {dims[0], dims[1], dims[2]};
+        std::vector<uint8_t> in = lbm::inside_grid(s, g);
+        std::memcpy(out, in.data(), in.size());
+    });
+}
+
+}  // extern "C"

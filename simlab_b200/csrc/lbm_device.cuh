@@ -1,0 +1,343 @@
+// Device-side building blocks of the D3Q19 time step: the velocity set,
+// population storage formats (FP32 / FP64 / FP16 / BF16 deviations from the
+// weights), stochastic rounding, launch parameters and record access.
+//
+// Reference semantics: crates/cfd/src/shader.rs (velocity set 22-60, record
+// layout 62-69, storage 147-162, stochastic rounding 507-517).
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace lbm {
+
+// ------------------------------------------------------------ velocity set
+// D3Q19 in the reference's order: rest, +-x, +-y, +-z, then the 12 edges
+// (shader.rs:22-42); opposite directions are neighbours (shader.rs:44-52).
+__host__ __device__ __forceinline__ constexpr int CX(int i) {
+    return (i == 1 || i == 7 || i == 9 || i == 13 || i == 15) ? 1 : ((i == 2 || i == 8 || i == 10 || i == 14 || i == 16) ? -1 : 0);
+}
+__host__ __device__ __forceinline__ constexpr int CY(int i) {
+    return (i == 3 || i == 7 || i == 11 || i == 14 || i == 17) ? 1 : ((i == 4 || i == 8 || i == 12 || i == 13 || i == 18) ? -1 : 0);
+}
+__host__ __device__ __forceinline__ constexpr int CZ(int i) {
+    return (i == 5 || i == 9 || i == 11 || i == 16 || i == 18) ? 1 : ((i == 6 || i == 10 || i == 12 || i == 15 || i == 17) ? -1 : 0);
+}
+__host__ __device__ __forceinline__ constexpr int OPP(int i) { return i == 0 ? 0 : ((i & 1) ? i + 1 : i - 1); }
+__host__ __device__ __forceinline__ constexpr double WD(int i) { return i == 0 ? 1.0 / 3.0 : (i <= 6 ? 1.0 / 18.0 : 1.0 / 36.0); }
+__host__ __device__ __forceinline__ constexpr int DIR(int x, int y, int z) {
+    int r = 0;
+    for (int i = 0; i < 19; i++)
+        if (CX(i) == x && CY(i) == y && CZ(i) == z) r = i;
+    return r;
+}
+
+// record layout (u32 words per wall record), shader.rs:62-69
+constexpr uint32_t RS = 40, R_MASK = 0, R_CELL = 1, R_Q = 2, R_FPOST = 11, R_MACRO = 29, R_FT = 33;
+// FP64 engine keeps the float fields of a record in doubles: 18 fpost, 4 macro, 6 ft
+constexpr uint32_t RD = 28, RD_FPOST = 0, RD_MACRO = 18, RD_FT = 22;
+
+constexpr int BLOCK = 256;
+
+// ------------------------------------------------------------ launch params
+template <class R>
+struct Consts {
+    R tau0, smag2, sponge_tau, sigma;
+    R sp_lo[3], sp_hi[3], u_inf[3], u_init[3], grav[3], center[3];
+};
+
+struct LatParams {
+    void *pop;                 // 19 * N stored populations, slot-major (d * N + cell)
+    uint32_t *flags;           // N words: 0 fluid, 1 solid, 2/3 face, (rec+1)<<2 wall cell
+    uint32_t *recs;            // nrec * RS words
+    double *recd;              // FP64 engine: nrec * RD doubles (else null)
+    const uint32_t *faces;     // face cells
+    const uint8_t *face_info;  // kind (0 velocity, 1 open, 2 free slip) | mirror axes << 2
+    double *partials;          // per wall block: 8 doubles
+    uint32_t *ticket;          // last-block counter of the force reduction
+    double *hist;              // per step slot: 8 doubles (F, T)
+    float4 *dump;              // macros() output
+    uint32_t NX, NY, NZ, N;
+    uint32_t nrec, nface;
+    int per[3];
+    int abs_u, total_p, wall_model, forcing, sponge_on, les_on, moving;
+    Consts<float> kf;
+    Consts<double> kd;
+};
+
+struct StepParams {
+    uint32_t seed;   // stochastic rounding seed of this step (lattice.rs:676)
+    uint32_t slot;   // history slot of this step
+    float omega[3];  // angular velocity, rad per step
+    double omega_d[3];
+    float rot[9];    // body axes in lattice coordinates, row-major (columns = axes)
+};
+
+template <class R> __device__ __forceinline__ const Consts<R> &K(const LatParams &p);
+template <> __device__ __forceinline__ const Consts<float> &K<float>(const LatParams &p) { return p.kf; }
+template <> __device__ __forceinline__ const Consts<double> &K<double>(const LatParams &p) { return p.kd; }
+
+// ------------------------------------------------------------ rounding
+// shader.rs:510-517: noise uniform in [-1/2, 1/2) of one unit in the last
+// place, from an integer hash of the slot key and the step seed.
+__device__ __forceinline__ uint32_t sr_hash(uint32_t key, uint32_t seed) {
+    uint32_t h = (key * 0x9E3779B1u) ^ (seed * 0x85EBCA77u + 0x632BE5ABu);
+    h ^= h >> 16; h *= 0x7feb352du; h ^= h >> 15; h *= 0x846ca68bu; h ^= h >> 16;
+    return h;
+}
+__device__ __forceinline__ float pow2i(int e) { return __uint_as_float((uint32_t)(e + 127) << 23); }  // 2^e, normal e
+
+__device__ __forceinline__ float sround16(float x, uint32_t key, uint32_t seed) {
+    float r = (float)(sr_hash(key, seed) >> 8) * (1.0f / 16777216.0f) - 0.5f;
+    int e = (int)((__float_as_uint(x) >> 23) & 0xffu) - 127;
+    float ulp = pow2i(max(e, -14) - 10);
+    float v = __fadd_rn(x, __fmul_rn(r, ulp));
+    return fminf(fmaxf(v, -65000.0f), 65000.0f);
+}
+__device__ __forceinline__ float sround_bf16(float x, uint32_t key, uint32_t seed) {
+    float r = (float)(sr_hash(key, seed) >> 8) * (1.0f / 16777216.0f) - 0.5f;
+    int e = (int)((__float_as_uint(x) >> 23) & 0xffu) - 127;
+    float ulp = pow2i(max(e, -126) - 7);
+    return __fadd_rn(x, __fmul_rn(r, ulp));
+}
+
+// ------------------------------------------------------------ storage
+// Every format stores f_i - w_i.  FP16 multiplies by 32768 first
+// (shader.rs:73, 153-162); BF16 keeps the value as is.
+template <class S> struct Pop;
+template <> struct Pop<float> {
+    using real = float;
+    static __device__ __forceinline__ float ld(const float *p) { return *p; }
+    static __device__ __forceinline__ void st(float *p, float v, uint32_t, uint32_t) { *p = v; }
+};
+template <> struct Pop<double> {
+    using real = double;
+    static __device__ __forceinline__ double ld(const double *p) { return *p; }
+    static __device__ __forceinline__ void st(double *p, double v, uint32_t, uint32_t) { *p = v; }
+};
+template <> struct Pop<__half> {
+    using real = float;
+    static __device__ __forceinline__ float ld(const __half *p) { return __half2float(*p) * (1.0f / 32768.0f); }
+    static __device__ __forceinline__ void st(__half *p, float v, uint32_t key, uint32_t seed) {
+        *p = __float2half_rn(sround16(v * 32768.0f, key, seed));
+    }
+};
+template <> struct Pop<__nv_bfloat16> {
+    using real = float;
+    static __device__ __forceinline__ float ld(const __nv_bfloat16 *p) { return __bfloat162float(*p); }
+    static __device__ __forceinline__ void st(__nv_bfloat16 *p, float v, uint32_t key, uint32_t seed) {
+        *p = __float2bfloat16_rn(sround_bf16(v, key, seed));
+    }
+};
+
+// ------------------------------------------------------------ records
+template <class R> struct Rec;
+template <> struct Rec<float> {
+    static __device__ __forceinline__ float fpost(const LatParams &p, uint32_t r, int i) { return __uint_as_float(p.recs[r * RS + R_FPOST + i - 1]); }
+    static __device__ __forceinline__ void set_fpost(const LatParams &p, uint32_t r, int i, float v) { p.recs[r * RS + R_FPOST + i - 1] = __float_as_uint(v); }
+    static __device__ __forceinline__ float macro(const LatParams &p, uint32_t r, int a) { return __uint_as_float(p.recs[r * RS + R_MACRO + a]); }
+    static __device__ __forceinline__ void set_macro(const LatParams &p, uint32_t r, int a, float v) { p.recs[r * RS + R_MACRO + a] = __float_as_uint(v); }
+    static __device__ __forceinline__ float ft(const LatParams &p, uint32_t r, int a) { return __uint_as_float(p.recs[r * RS + R_FT + a]); }
+    static __device__ __forceinline__ void set_ft(const LatParams &p, uint32_t r, int a, float v) { p.recs[r * RS + R_FT + a] = __float_as_uint(v); }
+};
+template <> struct Rec<double> {
+    static __device__ __forceinline__ double fpost(const LatParams &p, uint32_t r, int i) { return p.recd[r * RD + RD_FPOST + i - 1]; }
+    static __device__ __forceinline__ void set_fpost(const LatParams &p, uint32_t r, int i, double v) {
+        p.recd[r * RD + RD_FPOST + i - 1] = v;
+        p.recs[r * RS + R_FPOST + i - 1] = __float_as_uint((float)v);
+    }
+    static __device__ __forceinline__ double macro(const LatParams &p, uint32_t r, int a) { return p.recd[r * RD + RD_MACRO + a]; }
+    static __device__ __forceinline__ void set_macro(const LatParams &p, uint32_t r, int a, double v) {
+        p.recd[r * RD + RD_MACRO + a] = v;
+        p.recs[r * RS + R_MACRO + a] = __float_as_uint((float)v);
+    }
+    static __device__ __forceinline__ double ft(const LatParams &p, uint32_t r, int a) { return p.recd[r * RD + RD_FT + a]; }
+    static __device__ __forceinline__ void set_ft(const LatParams &p, uint32_t r, int a, double v) {
+        p.recd[r * RD + RD_FT + a] = v;
+        p.recs[r * RS + R_FT + a] = __float_as_uint((float)v);
+    }
+};
+
+// q of direction i (1..18) from the f16 pairs of a record
+__device__ __forceinline__ float rec_q(const uint32_t *recs, uint32_t r, int i) {
+    uint32_t w = recs[r * RS + R_Q + (i - 1) / 2];
+    uint16_t h = ((i - 1) & 1) ? (uint16_t)(w >> 16) : (uint16_t)(w & 0xffffu);
+    return __half2float(__ushort_as_half(h));
+}
+
+// ------------------------------------------------------------ neighbours
+// Offsets of the six axis neighbours with periodic wrap (shader.rs:247-252).
+struct Nb {
+    int32_t xp, xm, yp, ym, zp, zm;
+    __device__ __forceinline__ int32_t off(int dx, int dy, int dz) const {
+        return (dx == 1 ? xp : (dx == -1 ? xm : 0)) + (dy == 1 ? yp : (dy == -1 ? ym : 0)) + (dz == 1 ? zp : (dz == -1 ? zm : 0));
+    }
+};
+__device__ __forceinline__ Nb make_nb(const LatParams &p, uint32_t x, uint32_t y, uint32_t z) {
+    Nb b;
+    const int32_t nx = (int32_t)p.NX, nxy = (int32_t)(p.NX * p.NY);
+    b.xp = x == p.NX - 1 ? -(nx - 1) : 1;
+    b.xm = x == 0 ? (nx - 1) : -1;
+    b.yp = y == p.NY - 1 ? -(int32_t)(p.NY - 1) * nx : nx;
+    b.ym = y == 0 ? (int32_t)(p.NY - 1) * nx : -nx;
+    b.zp = z == p.NZ - 1 ? -(int32_t)(p.NZ - 1) * nxy : nxy;
+    b.zm = z == 0 ? (int32_t)(p.NZ - 1) * nxy : -nxy;
+    return b;
+}
+
+__device__ __forceinline__ void coords(const LatParams &p, uint32_t n, uint32_t &x, uint32_t &y, uint32_t &z) {
+    uint32_t nxy = p.NX * p.NY;
+    z = n / nxy;
+    uint32_t r = n - z * nxy;
+    y = r / p.NX;
+    x = r - y * p.NX;
+}
+
+// ------------------------------------------------------------ AA access
+// Input parity P (shader.rs:5-13): before a step of parity P the population
+// arriving at cell n in direction i sits at P=0: (n, i), P=1: (n - c_i, opp i);
+// the step writes its post-collision values to P=0: (n, opp i),
+// P=1: (n + c_i, i).
+template <class S, int P>
+__device__ __forceinline__ void load_in(const LatParams &p, uint32_t n, const Nb &nb, typename Pop<S>::real *f) {
+    const S *pop = (const S *)p.pop;
+    const size_t N = p.N;
+#pragma unroll
+    for (int i = 0; i < 19; i++) {
+        if (P == 0 || i == 0) f[i] = Pop<S>::ld(pop + (size_t)i * N + n);
+        else f[i] = Pop<S>::ld(pop + (size_t)OPP(i) * N + (uint32_t)((int32_t)n + nb.off(-CX(i), -CY(i), -CZ(i))));
+    }
+}
+
+template <class S, int P>
+__device__ __forceinline__ void store_out(const LatParams &p, uint32_t n, const Nb &nb, const typename Pop<S>::real *f, uint32_t seed) {
+    S *pop = (S *)p.pop;
+    const size_t N = p.N;
+    const uint32_t key0 = n * 19u;
+#pragma unroll
+    for (int i = 0; i < 19; i++) {
+        if (P == 0 || i == 0) Pop<S>::st(pop + (size_t)OPP(i) * N + n, f[i], key0 + (uint32_t)OPP(i), seed);
+        else Pop<S>::st(pop + (size_t)i * N + (uint32_t)((int32_t)n + nb.off(CX(i), CY(i), CZ(i))), f[i], key0 + (uint32_t)i, seed);
+    }
+}
+
+// the post-collision populations a cell wrote in the previous step of
+// parity Q (shader.rs:307-321)
+template <class S, int Q>
+__device__ __forceinline__ void load_prev_out(const LatParams &p, uint32_t n, const Nb &nb, typename Pop<S>::real *f) {
+    const S *pop = (const S *)p.pop;
+    const size_t N = p.N;
+#pragma unroll
+    for (int i = 0; i < 19; i++) {
+        if (Q == 0 || i == 0) f[i] = Pop<S>::ld(pop + (size_t)OPP(i) * N + n);
+        else f[i] = Pop<S>::ld(pop + (size_t)i * N + (uint32_t)((int32_t)n + nb.off(CX(i), CY(i), CZ(i))));
+    }
+}
+
+// writes a face cell's "previous" post-collision populations for parity Q,
+// skipping targets that leave a non-periodic domain (shader.rs:273-305)
+template <class S, int Q>
+__device__ __forceinline__ void store_prev_out(const LatParams &p, uint32_t n, uint32_t x, uint32_t y, uint32_t z, const Nb &nb,
+                                               const typename Pop<S>::real *f, uint32_t seed) {
+    S *pop = (S *)p.pop;
+    const size_t N = p.N;
+    const uint32_t key0 = n * 19u;
+#pragma unroll
+    for (int i = 0; i < 19; i++) {
+        if (Q == 0 || i == 0) {
+            Pop<S>::st(pop + (size_t)OPP(i) * N + n, f[i], key0 + (uint32_t)OPP(i), seed);
+        } else {
+            bool ok = true;
+            if (CX(i) == 1) ok = ok && (p.per[0] || x < p.NX - 1);
+            if (CX(i) == -1) ok = ok && (p.per[0] || x > 0);
+            if (CY(i) == 1) ok = ok && (p.per[1] || y < p.NY - 1);
+            if (CY(i) == -1) ok = ok && (p.per[1] || y > 0);
+            if (CZ(i) == 1) ok = ok && (p.per[2] || z < p.NZ - 1);
+            if (CZ(i) == -1) ok = ok && (p.per[2] || z > 0);
+            if (ok) Pop<S>::st(pop + (size_t)i * N + (uint32_t)((int32_t)n + nb.off(CX(i), CY(i), CZ(i))), f[i], key0 + (uint32_t)i, seed);
+        }
+    }
+}
+
+// ------------------------------------------------------------ projections
+template <class R>
+__device__ __forceinline__ R cdot(int i, R ux, R uy, R uz) {
+    R t = 0;
+    if (CX(i) == 1) t = t + ux; else if (CX(i) == -1) t = t - ux;
+    if (CY(i) == 1) t = t + uy; else if (CY(i) == -1) t = t - uy;
+    if (CZ(i) == 1) t = t + uz; else if (CZ(i) == -1) t = t - uz;
+    return t;
+}
+
+// shifted equilibrium w (rho1 + rho (3cu + 4.5cu^2 - 1.5u^2)), shader.rs:367-377
+template <class R>
+__device__ __forceinline__ R feq_i(int i, R rho1, R rho, R ux, R uy, R uz, R usq) {
+    R cu = cdot<R>(i, ux, uy, uz);
+    return (R)WD(i) * (rho1 + rho * ((R)3 * cu + (R)4.5 * cu * cu - usq));
+}
+
+// 4.5 w (c c : Pi - tr Pi / 3), shader.rs:379-396; pi = xx yy zz xy xz yz
+template <class R>
+__device__ __forceinline__ R fneq_i(int i, const R *pi, R tr) {
+    R t = -tr;
+    if (CX(i) != 0) t = t + pi[0];
+    if (CY(i) != 0) t = t + pi[1];
+    if (CZ(i) != 0) t = t + pi[2];
+    if (CX(i) * CY(i) != 0) t = t + (R)(2 * CX(i) * CY(i)) * pi[3];
+    if (CX(i) * CZ(i) != 0) t = t + (R)(2 * CX(i) * CZ(i)) * pi[4];
+    if (CY(i) * CZ(i) != 0) t = t + (R)(2 * CY(i) * CZ(i)) * pi[5];
+    return (R)(4.5 * WD(i)) * t;
+}
+
+template <class R>
+struct Moments {
+    R rho1, jx, jy, jz, sxx, syy, szz, sxy, sxz, syz;
+};
+
+template <class R>
+__device__ __forceinline__ Moments<R> moments(const R *f) {
+    Moments<R> m{};
+#pragma unroll
+    for (int i = 0; i < 19; i++) {
+        m.rho1 += f[i];
+        if (CX(i)) m.jx += (R)CX(i) * f[i];
+        if (CY(i)) m.jy += (R)CY(i) * f[i];
+        if (CZ(i)) m.jz += (R)CZ(i) * f[i];
+        if (CX(i)) m.sxx += f[i];
+        if (CY(i)) m.syy += f[i];
+        if (CZ(i)) m.szz += f[i];
+        if (CX(i) * CY(i)) m.sxy += (R)(CX(i) * CY(i)) * f[i];
+        if (CX(i) * CZ(i)) m.sxz += (R)(CX(i) * CZ(i)) * f[i];
+        if (CY(i) * CZ(i)) m.syz += (R)(CY(i) * CZ(i)) * f[i];
+    }
+    return m;
+}
+
+// shader.rs:818-824: non-equilibrium stress from shifted moments
+template <class R>
+__device__ __forceinline__ void pi_neq(const Moments<R> &m, R rho, R ux, R uy, R uz, R *pi) {
+    pi[0] = m.sxx - rho * ux * ux - m.rho1 / (R)3;
+    pi[1] = m.syy - rho * uy * uy - m.rho1 / (R)3;
+    pi[2] = m.szz - rho * uz * uz - m.rho1 / (R)3;
+    pi[3] = m.sxy - rho * ux * uy;
+    pi[4] = m.sxz - rho * ux * uz;
+    pi[5] = m.syz - rho * uy * uz;
+}
+
+// shader.rs:528-538
+template <class R>
+__device__ __forceinline__ R sponge_at(const Consts<R> &k, const LatParams &p, uint32_t x, uint32_t y, uint32_t z) {
+    R pos[3] = {(R)x, (R)y, (R)z};
+    R hi[3] = {(R)(p.NX - 1) - pos[0], (R)(p.NY - 1) - pos[1], (R)(p.NZ - 1) - pos[2]};
+    R s = 0;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        if (k.sp_lo[a] > (R)0) s = max(s, (R)1 - pos[a] / k.sp_lo[a]);
+        if (k.sp_hi[a] > (R)0) s = max(s, (R)1 - hi[a] / k.sp_hi[a]);
+    }
+    return min(max(s, (R)0), (R)1);
+}
+
+}  // namespace lbm

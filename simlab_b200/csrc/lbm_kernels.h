@@ -1,0 +1,19 @@
+// Kernel launchers of the D3Q19 time step (d3q19_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "lbm_device.cuh"
+
+namespace lbm {
+
+// storage: 0 FP32, 1 FP16, 2 BF16, 3 FP64 (lbm_storage); coll: 0 regularized, 1 BGK
+// ev: null, or 4 events recorded before faces, before walls, before bulk, after bulk
+cudaError_t launch_step(int storage, const LatParams &p, const StepParams &s, int parity, int coll, cudaStream_t st,
+                        cudaEvent_t *ev = nullptr);
+cudaError_t launch_init(int storage, const LatParams &p, cudaStream_t st);
+cudaError_t launch_dump(int storage, const LatParams &p, int q, cudaStream_t st);
+cudaError_t launch_sample(int storage, const LatParams &p, const StepParams &s, int q, const float *verts, uint32_t nvert, float voff,
+                          double *vacc, const int32_t *slicedef, uint32_t nslices, uint32_t npix, double *sacc, cudaStream_t st);
+cudaError_t launch_mass(int storage, const LatParams &p, int q, double *mass, unsigned long long *bad, cudaStream_t st);
+
+}  // namespace lbm

@@ -1,0 +1,37 @@
+// Host voxelizer types (crates/cfd/src/voxel.rs restated in C++).
+#pragma once
+#include <array>
+#include <cstddef>
+#include <cstdint>
+#include <vector>
+
+namespace lbm {
+
+struct Surface {  // voxel.rs:24-29
+    std::vector<std::array<double, 3>> verts;
+    std::vector<std::array<uint32_t, 3>> tris;
+};
+
+struct GridSpec {  // voxel.rs:49-66: points origin + h * (i, j, k)
+    std::array<double, 3> origin{};
+    double h = 1.0;
+    std::array<size_t, 3> dims{};
+};
+
+struct WallCell {  // voxel.rs:328-335
+    uint32_t cell = 0;
+    uint32_t mask = 0;
+    std::array<float, 27> q{};
+};
+
+struct StaticVoxels {  // voxel.rs:337-344
+    std::vector<uint32_t> solid;
+    std::vector<WallCell> walls;
+    std::array<size_t, 3> lo{}, hi{};
+};
+
+std::vector<uint8_t> inside_grid(const Surface &s, const GridSpec &g);
+bool seg_tri(const double o[3], const double d[3], const double t0[3], const double t1[3], const double t2[3], double *t);
+StaticVoxels voxelize_static(const Surface &s, std::array<size_t, 3> dims, int lattice);
+
+}  // namespace lbm

@@ -1,0 +1,253 @@
+"""CUDA engine (through the C ABI) against the CPU oracle and the reference's
+known answers.  Tolerances: FP32 relative L2 of the velocity <= 1e-5 after
+1000 steps (the reference's FP32 update restated); FP64 engine vs FP64
+oracle <= 1e-11; stochastic-rounding FP16/BF16 storage against the oracle
+with the same storage within the rounding noise (FP16 <= 2e-3, BF16 <= 2e-2
+relative L2 of the velocity deviation from the free stream)."""
+import numpy as np
+import pytest
+
+from oracle import OracleLattice
+from simlab_b200.cases import sphere_cd, sphere_re40
+from simlab_b200.lbm import Collision, FaceBc, Lattice, LatticeSetup, LbmError, Probes, SliceDef, StepIn, Storage, halfway, steps_array, voxelize_static
+from simlab_b200.shapes import sphere
+
+from helpers import ball, channel_case, momentum_setup, poiseuille_error, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _u(m):
+    return np.asarray(m)[:, 1:4].astype(np.float64)
+
+
+def _rho(m):
+    return np.asarray(m)[:, 0].astype(np.float64)
+
+
+def feature_case(storage=Storage.FP32, collision=Collision.REGULARIZED, wall_model=False):
+    """Every D3Q19 feature on a small grid: Bouzidi (interpolated q) sphere,
+    Smagorinsky, sponges + absorbing layers, total-pressure inlet, open and
+    free-slip faces, body force, spinning-wall velocity on static links."""
+    dims = (40, 30, 24)
+    c = (14.3, 15.2, 11.7)
+    v, t = sphere(list(c), 5.3, 4)
+    vox = voxelize_static(v, t, list(dims))
+    F = FaceBc
+    st = LatticeSetup(dims=list(dims), faces=[F.VELOCITY, F.OPEN, F.FREE_SLIP, F.OPEN, F.FREE_SLIP, F.FREE_SLIP], nu=0.004,
+                      smagorinsky=0.17, u_inf=[0.05, 0.005, 0.0], u_init=[0.04, 0.0, 0.002], body_force=[1e-6, 0.0, -2e-7],
+                      sponge=[4, 6, 3, 3, 0, 2], sponge_tau=0.9, sponge_sigma=0.1, absorb_velocity=True, total_pressure_inlet=True,
+                      storage=storage, center=list(c), debug_dump=True, wall_model=wall_model, collision=collision)
+    return st, vox
+
+
+def spin_steps(n, w=(0.0, 0.0, 0.004)):
+    a = steps_array(n)
+    a["omega"] = np.asarray(w)
+    return a
+
+
+def _pair(st, vox, real64=False):
+    return Lattice(st, vox), OracleLattice(st, vox, real64=real64)
+
+
+def test_init_matches_oracle():
+    st, vox = feature_case()
+    g, o = _pair(st, vox)
+    mg, mo = g.macros(), o.macros()
+    assert np.array_equal(np.isnan(mg[:, 0]), np.isnan(mo[:, 0]))
+    assert rel_l2(_u(mg), _u(mo)) < 1e-6
+    assert np.array_equal(g.records(), o.records())
+
+
+def test_sphere_re40_fp32_parity_1000_steps():
+    """The 96x48x48 sphere case: relative L2 of u <= 1e-5 after 1000 steps."""
+    st, vox = sphere_re40(Storage.FP32)
+    g, o = _pair(st, vox)
+    hg, ho = g.run(1000), o.run(1000)
+    mg, mo = g.macros(), o.macros()
+    assert rel_l2(_u(mg), _u(mo)) <= 1e-5
+    assert rel_l2(_rho(mg) - 1.0, _rho(mo) - 1.0) <= 1e-4
+    cg, co = sphere_cd(hg[:, 0]), sphere_cd(ho[:, 0])
+    assert abs(cg[-1] / co[-1] - 1.0) < 1e-5
+    assert np.max(np.abs(hg - ho)) < 1e-5 * np.max(np.abs(ho))
+
+
+@pytest.mark.parametrize("collision", [Collision.REGULARIZED, Collision.BGK])
+@pytest.mark.parametrize("wall_model", [False, True])
+def test_feature_case_fp32_parity(collision, wall_model):
+    st, vox = feature_case(Storage.FP32, collision, wall_model)
+    g, o = _pair(st, vox)
+    steps = spin_steps(151)
+    hg, ho = g.run(steps), o.run(steps)
+    mg, mo = g.macros(), o.macros()
+    assert np.array_equal(np.isnan(mg[:, 0]), np.isnan(mo[:, 0]))
+    assert rel_l2(_u(mg), _u(mo)) <= 1e-5
+    assert np.max(np.abs(hg - ho)) <= 1e-5 * np.max(np.abs(ho)) + 1e-9
+    rg = g.records().view(np.float32).reshape(-1, 40)
+    ro = o.records().view(np.float32).reshape(-1, 40)
+    assert np.array_equal(g.records().reshape(-1, 40)[:, :11], o.records().reshape(-1, 40)[:, :11])
+    assert np.max(np.abs(rg[:, 11:33] - ro[:, 11:33])) < 1e-5
+
+
+def test_fp64_engine_matches_fp64_oracle():
+    st, vox = feature_case(Storage.FP64)
+    g, o = _pair(st, vox, real64=True)
+    steps = spin_steps(120)
+    hg, ho = g.run(steps), o.run(steps)
+    assert rel_l2(_u(g.macros()), _u(o.macros())) < 1e-6  # macros() readback is float32
+    assert np.max(np.abs(hg - ho)) <= 1e-11 * np.max(np.abs(ho))
+
+
+@pytest.mark.parametrize("storage,tol", [(Storage.FP16, 2e-3), (Storage.BF16, 2e-2)])
+def test_reduced_storage_parity(storage, tol):
+    st, vox = feature_case(storage)
+    g, o = _pair(st, vox)
+    hg, ho = g.run(100), o.run(100)
+    ug, uo = _u(g.macros()), _u(o.macros())
+    uinf = np.array([0.05, 0.005, 0.0])
+    assert rel_l2(ug - uinf, uo - uinf) <= tol
+    assert abs(hg[-1, 0] / ho[-1, 0] - 1.0) < 10 * tol
+
+
+def test_periodic_wraps_both_parities():
+    """Fully periodic box with a body force: the AA wrap at every face."""
+    n = 20
+    st = momentum_setup(n, 0.05, 0.02, 2e-6, [FaceBc.PERIODIC] * 6)
+    vox = ball(n, 4.0)
+    g, o = _pair(st, vox)
+    for _ in range(3):
+        hg, ho = g.run(33), o.run(33)
+        assert rel_l2(_u(g.macros()), _u(o.macros())) <= 1e-5
+        assert np.max(np.abs(hg - ho)) <= 1e-5 * np.max(np.abs(ho))
+
+
+def test_checkpoint_round_trip_is_exact():
+    st, vox = feature_case(Storage.FP16)
+    g = Lattice(st, vox)
+    g.run(17)
+    blob = g.save_state()
+    a = g.run(spin_steps(23))
+    g.load_state(blob)
+    assert g.steps_done == 17
+    b = g.run(spin_steps(23))
+    assert np.array_equal(a, b)
+
+
+def test_macros_needs_debug_dump():
+    st, vox = feature_case()
+    st.debug_dump = False
+    g = Lattice(st, vox)
+    with pytest.raises(LbmError, match="debug_dump"):
+        g.macros()
+
+
+def test_mass_and_finiteness():
+    st = momentum_setup(24, 0.05, 0.01, 0.0, [FaceBc.PERIODIC] * 6)
+    g = Lattice(st, ball(24, 4.0))
+    m0, bad0 = g.mass()
+    g.run(200)
+    m1, bad1 = g.mass()
+    assert bad0 == 0 and bad1 == 0
+    assert abs(m1 / m0 - 1.0) < 1e-6
+
+
+def test_slice_and_vertex_sampling():
+    st, vox = sphere_re40(Storage.FP32)
+    probes = Probes(verts=[([7.0, 0.0, 0.0], [1.0, 0.0, 0.0]), ([0.0, -7.0, 0.0], [0.0, -1.0, 0.0])],
+                    slices=[SliceDef(origin=[0, 0, 24], u=[1, 0, 0], v=[0, 1, 0], nu=96, nv=48)], vertex_offset=1.0)
+    g = Lattice(st, vox, probes)
+    g.run(50)
+    g.reset_samples()
+    g.run([StepIn.still(True)] * 3)
+    sm = g.slice_means()
+    vm = g.vertex_means()
+    m = g.macros()
+    idx = (24 * 48 + np.arange(48)[:, None]) * 96 + np.arange(96)[None, :]
+    ref = m[idx.ravel()]
+    ok = ~np.isnan(ref[:, 0])
+    assert np.all(np.isnan(sm[~ok, 0]))
+    # the mean over three steps is close to the last step's field
+    assert np.max(np.abs(sm[ok, 1] - ref[ok, 1])) < 2e-3
+    assert np.all(np.isfinite(vm)) and np.all(np.abs(vm - 1.0) < 0.02)
+
+
+# ------------------------------------------------------------------ known answers on the GPU
+def test_gpu_poiseuille_second_order():
+    errs = []
+    for h in (8.0, 16.0, 32.0):
+        st, vox, steps, params = channel_case(h, 0.02, Storage.FP32)
+        g = Lattice(st, vox)
+        hist = g.run(steps)
+        e, bal = poiseuille_error(g.macros(), hist, params)
+        assert abs(bal) < 2e-3
+        errs.append(e)
+    assert errs[2] < 2e-3 and (np.log2(errs[1] / errs[2]) > 1.6 or errs[2] < 1e-4)
+
+
+@pytest.mark.parametrize("storage,tol", [(Storage.FP16, 3e-3), (Storage.BF16, 2e-2)])
+def test_gpu_poiseuille_reduced_storage(storage, tol):
+    for umax in (0.02, 0.06):
+        st, vox, steps, params = channel_case(16.0, umax, storage)
+        g = Lattice(st, vox)
+        hist = g.run(steps)
+        e, bal = poiseuille_error(g.macros(), hist, params)
+        assert e < tol, e
+
+
+def test_gpu_momentum_balance():
+    n = 40
+    g = Lattice(momentum_setup(n, 0.05, 0.05, 0.0, [FaceBc.PERIODIC] * 6), ball(n, 6.0))
+
+    def pm():
+        m = g.macros().astype(np.float64)
+        ok = ~np.isnan(m[:, 0])
+        return float(np.sum(m[ok, 0] * m[ok, 1]))
+
+    p0 = pm()
+    h = g.run(600)
+    p1 = pm()
+    imp = float(h[:, 0].sum())
+    assert imp > 0 and abs((p0 - p1 - imp) / imp) < 5e-3
+
+
+def test_gpu_uniform_state_no_force():
+    n = 32
+    g = Lattice(momentum_setup(n, 0.05, 0.0, 0.0, [FaceBc.OPEN] * 6), ball(n, 5.0))
+    assert np.all(np.abs(g.run(50)) < 1e-4)
+
+
+def test_gpu_periodic_sphere_array_stokes_drag():
+    """momentum.rs:53-71: Hasimoto / Sangani-Acrivos K within 4 %."""
+    n, r, nu, gr = 48, 6.0, 1.0 / 6.0, 1e-7
+    g = Lattice(momentum_setup(n, nu, 0.0, gr, [FaceBc.PERIODIC] * 6), ball(n, r))
+    steps = int(4.0 * n * n / nu)
+    h = g.run(steps)
+    vol = float(n) ** 3
+    m = g.macros().astype(np.float64)
+    ok = ~np.isnan(m[:, 0])
+    ux = float(np.sum(m[ok, 0] * m[ok, 1])) / vol
+    f = h[-1, 0]
+    c = 4.0 / 3.0 * np.pi * r ** 3 / vol
+    k_ref = 1.0 / (1.0 - 1.7601 * c ** (1 / 3) + c - 1.5593 * c * c + 3.9799 * c ** (8 / 3) - 3.0734 * c ** (10 / 3))
+    k = f / (6.0 * np.pi * nu * r * ux)
+    assert abs(k / k_ref - 1.0) < 0.04, (k, k_ref)
+
+
+# ------------------------------------------------------------------ full size
+def test_arm_les_full_size_fp16_runs_finite():
+    """The 512x256x256 LES arm in FP16: finite forces and densities, and the
+    FP16 drag follows the FP32 engine's early transient within 0.5 %."""
+    from simlab_b200.cases import arm_les
+
+    out = {}
+    for s in (Storage.FP16, Storage.FP32):
+        st, vox = arm_les(s)
+        g = Lattice(st, vox)
+        h = g.run(300)
+        mass, bad = g.mass()
+        assert bad == 0 and np.all(np.isfinite(h))
+        out[s] = h
+        g.close()
+    fx16, fx32 = out[Storage.FP16][-50:, 0].mean(), out[Storage.FP32][-50:, 0].mean()
+    assert abs(fx16 / fx32 - 1.0) < 5e-3, (fx16, fx32)
