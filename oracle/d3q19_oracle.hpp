@@ -127,11 +127,12 @@ inline float sround16(float x, uint32_t key, uint32_t seed) {
     float v = x + r * ulp;
     return std::min(std::max(v, -65000.0f), 65000.0f);
 }
-// BF16 variant: one bfloat16 ulp (8 significant bits); no scaling, no clamp.
+// BF16 variant: one bfloat16 ulp (8 significant bits), exponent floored at
+// -119 so the ulp is a normal float; no scaling, no clamp.
 inline float sround_bf16(float x, uint32_t key, uint32_t seed) {
     float r = (float)(sr_hash(key, seed) >> 8) * (1.0f / 16777216.0f) - 0.5f;
     int e = (int)((fbits(x) >> 23) & 0xffu) - 127;
-    float ulp = std::ldexp(1.0f, std::max(e, -126) - 7);
+    float ulp = std::ldexp(1.0f, std::max(e, -119) - 7);
     return x + r * ulp;
 }
 
@@ -471,10 +472,10 @@ struct D3Q19 {
                 double usq = 1.5 * (st.u_init[0] * st.u_init[0] + st.u_init[1] * st.u_init[1] + st.u_init[2] * st.u_init[2]);
                 for (int i = 1; i < 19; i++) {
                     double cu = C19[i][0] * st.u_init[0] + C19[i][1] * st.u_init[1] + C19[i][2] * st.u_init[2];
-                    rc.fpost[i] = (Real)(float)(weight19(i) * (3.0 * cu + 4.5 * cu * cu - usq));
+                    rc.fpost[i] = (Real)(weight19(i) * (3.0 * cu + 4.5 * cu * cu - usq));  // f32 record word in FP32
                 }
-                rc.macro[0] = (Real)1.0f;
-                for (int k = 0; k < 3; k++) rc.macro[1 + k] = (Real)(float)st.u_init[k];
+                rc.macro[0] = (Real)1.0;
+                for (int k = 0; k < 3; k++) rc.macro[1 + k] = (Real)st.u_init[k];
                 recs.push_back(rc);
                 rec_of.push_back({w.cell, (uint32_t)r + 1});
             }
@@ -647,7 +648,7 @@ struct D3Q19 {
     std::array<double, 6> step(const lbm_step_in &sin) {
         int p = (int)(steps_done % 2);
         seed = (uint32_t)steps_done * 2654435761u;  // lattice.rs:676
-        Real omega[3] = {(Real)(float)sin.omega[0], (Real)(float)sin.omega[1], (Real)(float)sin.omega[2]};
+        Real omega[3] = {(Real)sin.omega[0], (Real)sin.omega[1], (Real)sin.omega[2]};
         if (!faces.empty()) faces_step(p);
 #pragma omp parallel for schedule(static)
         for (long long n = 0; n < (long long)N; n++) main_cell((uint64_t)n, p, omega);

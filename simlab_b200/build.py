@@ -22,7 +22,8 @@ CXX_SOURCES = ["voxel.cpp"]
 HEADERS = ["lbm_device.cuh", "lbm_kernels.h", "voxel.hpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-fopenmp", "-Xptxas", "-v"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-prec-div=false", "-prec-sqrt=false", "-Xcompiler", "-fPIC,-fopenmp",
+              "-Xptxas", "-v"]
 
 
 def nvcc() -> str:

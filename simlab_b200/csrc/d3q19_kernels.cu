@@ -16,7 +16,9 @@
 // ordering between them.  The population layout is the reference's
 // slot-major SoA (shader.rs:147-152): direction d of cell n at d * N + n,
 // stored as f - w (FP32, FP64, FP16 x 32768 with stochastic rounding, BF16).
+#include <algorithm>
 #include <cstdio>
+#include <type_traits>
 #include <utility>
 
 #include "lbm_device.cuh"
@@ -86,23 +88,44 @@ __device__ R wall_tau(const LatParams &p, const Consts<R> &k, uint32_t r, uint32
 }
 
 // One cell's update after its populations f are loaded (and wall links
-// applied).  Returns rho and u (the u written to wall records).
-template <class R, int COLL>
+// applied): shader.rs:815-847 (regularized; plain BGK relaxes f itself and
+// omits the forcing's regularization correction).  Returns rho and u (the u
+// written to wall records).
+//
+// SC is the storage scale: f holds SC * (f_i - w_i) on entry and receives the
+// post-collision values in the same units (SC = 32768 for FP16 storage, 1
+// otherwise).  Scaling by a power of two is exact, so the moments equal those
+// of the unscaled populations bit for bit, and the scale of the outputs rides
+// on compile-time weights.
+//
+// The 9 opposite pairs (i = 2k+1, o = 2k+2) share c c, so the equilibrium,
+// the non-equilibrium projection, the absorbing target and the forcing term
+// are each split into a part even in c (the same for i and o) and a part odd
+// in c (opposite signs); with per-weight-class coefficients a pair costs a
+// handful of instructions.
+template <class R, int COLL, int SC = 1>
 __device__ __forceinline__ void relax(const LatParams &p, const Consts<R> &k, R *f, uint32_t x, uint32_t y, uint32_t z,
                                       bool wall, uint32_t r, uint32_t mask, R pcx, R pcy, R pcz, const R *om, R &rho_o, R &ux_o,
                                       R &uy_o, R &uz_o) {
-    const Moments<R> m = moments<R>(f);
+    const R isc = (R)(1.0 / SC);
+    Moments<R> m = moments<R>(f);
+    if (SC != 1) {
+        m.rho1 *= isc; m.jx *= isc; m.jy *= isc; m.jz *= isc;
+        m.sxx *= isc; m.syy *= isc; m.szz *= isc; m.sxy *= isc; m.sxz *= isc; m.syz *= isc;
+    }
     const R rho = (R)1 + m.rho1;
-    const R ux = m.jx / rho + (R)0.5 * k.grav[0];
-    const R uy = m.jy / rho + (R)0.5 * k.grav[1];
-    const R uz = m.jz / rho + (R)0.5 * k.grav[2];
+    const R irho = (R)1 / rho;
+    const R ux = m.jx * irho + (R)0.5 * k.grav[0];
+    const R uy = m.jy * irho + (R)0.5 * k.grav[1];
+    const R uz = m.jz * irho + (R)0.5 * k.grav[2];
     R pi[6];
     pi_neq<R>(m, rho, ux, uy, uz, pi);
     R tau = k.tau0;
     if (p.les_on) {
-        R pp = pi[0] * pi[0] + pi[1] * pi[1] + pi[2] * pi[2] + (R)2 * (pi[3] * pi[3] + pi[4] * pi[4] + pi[5] * pi[5]);
-        R qn = sqrt((R)2 * pp);
-        tau = (R)0.5 * (k.tau0 + sqrt(k.tau0 * k.tau0 + (R)18 * k.smag2 * qn / rho));
+        // Smagorinsky tau from |Pi_neq| (shader.rs:825-828)
+        const R pp = pi[0] * pi[0] + pi[1] * pi[1] + pi[2] * pi[2] + (R)2 * (pi[3] * pi[3] + pi[4] * pi[4] + pi[5] * pi[5]);
+        const R qn = sqrt((R)2 * pp);
+        tau = (R)0.5 * (k.tau0 + sqrt(k.tau0 * k.tau0 + (R)18 * k.smag2 * qn * irho));
     }
     if (wall && p.wall_model && mask != 0u) tau = wall_tau<R>(p, k, r, mask, pcx, pcy, pcz, ux, uy, uz, tau, om);
     R sp = 0;
@@ -111,12 +134,9 @@ __device__ __forceinline__ void relax(const LatParams &p, const Consts<R> &k, R 
         if (sp > (R)0 && k.sponge_tau > tau) tau = tau + sp * sp * (k.sponge_tau - tau);
     }
     const R omg = (R)1 / tau;
+    const R om1 = (R)1 - omg;
     const R usq = (R)1.5 * (ux * ux + uy * uy + uz * uz);
-    const bool absorb = p.sponge_on && sp > (R)0 && k.sigma > (R)0;
-    R atx = ux, aty = uy, atz = uz;
-    if (p.abs_u) { atx = k.u_inf[0]; aty = k.u_inf[1]; atz = k.u_inf[2]; }
-    const R ausq = (R)1.5 * (atx * atx + aty * aty + atz * atz);
-    const R sg = k.sigma * sp * sp;
+    const R sg = k.sigma * sp * sp;  // absorbing strength (0 outside the layers)
     const R tr = (pi[0] + pi[1] + pi[2]) * (R)(1.0 / 3.0);
     R Gx = 0, Gy = 0, Gz = 0, uG = 0, fo = 0;
     if (p.forcing) {
@@ -124,23 +144,89 @@ __device__ __forceinline__ void relax(const LatParams &p, const Consts<R> &k, R 
         uG = ux * Gx + uy * Gy + uz * Gz;
         fo = (R)1 - (R)0.5 * omg;
     }
+    // The equilibrium is fe_i = even + odd with even = A cu^2 + B, odd = O cu
+    // (per weight class a: 1/18, e: 1/36, all scaled by SC).  The absorbing
+    // layer adds sg (ft_i - fe_i) (shader.rs:838-845), linear in the same
+    // basis: with ft = feq(0, u) it is -sg rho1 w (1 - 1.5u^2 + 4.5cu^2 + 3cu);
+    // with ft = feq(0, u_inf) it is sg ft_i - sg fe_i.  Folding it into the
+    // coefficients leaves the per-pair cost unchanged:
+    //   regularized: v = fe + (1 - omega) fneq + delta
+    //   BGK:         v = (1 - omega) f + omega fe + delta
+    const R wa = (R)(SC / 18.0), we = (R)(SC / 36.0), w0 = (R)(SC / 3.0);
+    const R Bq = m.rho1 - rho * usq;
+    const R lam = COLL == 1 ? omg : (R)1;
+    R cA, cB, cO, dB;  // coefficient multipliers (unit weight) and the constant shift
+    if (p.abs_u) {
+        const R l2 = lam - sg;
+        cA = l2 * (R)4.5 * rho;
+        cB = l2 * Bq;
+        cO = l2 * (R)3 * rho;
+        dB = 0;
+    } else {
+        const R sr = sg * m.rho1;
+        cA = (R)4.5 * (lam * rho - sr);
+        cB = lam * Bq;
+        dB = -sr * ((R)1 - usq);
+        cO = (R)3 * (lam * rho - sr);
+    }
+    const R sgsc = sg * (R)SC;  // for the u_inf target, in storage units
+    const R A_a = wa * cA, A_e = we * cA, B_a = wa * (cB + dB), B_e = we * (cB + dB), O_a = wa * cO, O_e = we * cO;
+    const R Cn_a = (R)4.5 * wa * om1, Cn_e = (R)4.5 * we * om1;
+    // c c : Pi - tr for edges = (Pi_aa - tr/2) + (Pi_bb - tr/2) + 2 s Pi_ab
+    const R ht = (R)0.5 * tr;
+    const R qx = pi[0] - ht, qy = pi[1] - ht, qz = pi[2] - ht;
+    // rest population
+    {
+        R v = w0 * (cB + dB);
+        if (COLL == 1) v = v + om1 * f[0];
+        else v = v - ((R)4.5 * w0 * om1) * tr;
+        if (p.abs_u) v = v + sgsc * k.ft_rest;
+        if (p.forcing) v = v + w0 * (fo * ((R)-3 * uG));
+        f[0] = v;
+    }
 #pragma unroll
-    for (int i = 0; i < 19; i++) {
-        const R fe = feq_i<R>(i, m.rho1, rho, ux, uy, uz, usq);
-        R v;
-        if (COLL == 1) v = f[i] - omg * (f[i] - fe);                 // plain BGK
-        else v = fe + ((R)1 - omg) * fneq_i<R>(i, pi, tr);           // regularized
-        if (absorb) {
-            const R ft = feq_i<R>(i, (R)0, (R)1, atx, aty, atz, ausq);
-            v = v + sg * (ft - fe);
+    for (int kk = 0; kk < 9; kk++) {
+        const int i = 2 * kk + 1, o = i + 1;
+        const bool axis = kk < 3;
+        const R cu = cdot<R>(i, ux, uy, uz);
+        R even = (axis ? A_a : A_e) * (cu * cu) + (axis ? B_a : B_e);
+        R odd = (axis ? O_a : O_e) * cu;
+        if (p.abs_u) {
+            even = even + sgsc * k.ft_even[kk];
+            odd = odd + sgsc * k.ft_odd[kk];
+        }
+        R vi, vo;
+        if (COLL == 1) {
+            const R ei = even + om1 * f[i], eo = even + om1 * f[o];
+            vi = ei + odd;
+            vo = eo - odd;
+        } else {
+            R ccp;  // c c : Pi - tr
+            if (kk == 0) ccp = pi[0] - tr;
+            else if (kk == 1) ccp = pi[1] - tr;
+            else if (kk == 2) ccp = pi[2] - tr;
+            else {
+                const R a1 = CX(i) ? qx : qy;
+                const R a2 = CZ(i) ? qz : qy;
+                const R pab = (CX(i) && CY(i)) ? pi[3] : ((CX(i) && CZ(i)) ? pi[4] : pi[5]);
+                const int sgn = CX(i) * CY(i) + CX(i) * CZ(i) + CY(i) * CZ(i);
+                ccp = (a1 + a2) + (R)(2 * sgn) * pab;
+            }
+            const R en = even + (axis ? Cn_a : Cn_e) * ccp;
+            vi = en + odd;
+            vo = en - odd;
         }
         if (p.forcing) {
-            const R cu = cdot<R>(i, ux, uy, uz), cg = cdot<R>(i, Gx, Gy, Gz);
-            R t = fo * ((R)3 * (cg - uG) + (R)9 * cu * cg);
-            if (COLL != 1) t = t - (R)1.5 * ((R)1 - omg) * cg;
-            v = v + (R)WD(i) * t;
+            const R w = axis ? wa : we;
+            const R cg = cdot<R>(i, Gx, Gy, Gz);
+            const R fe_ = w * (fo * ((R)9 * cu * cg - (R)3 * uG));
+            R fod = w * (fo * (R)3 * cg);
+            if (COLL != 1) fod = fod - w * ((R)1.5 * om1 * cg);
+            vi = vi + (fe_ + fod);
+            vo = vo + (fe_ - fod);
         }
-        f[i] = v;
+        f[i] = vi;
+        f[o] = vo;
     }
     rho_o = rho; ux_o = ux; uy_o = uy; uz_o = uz;
 }
@@ -162,7 +248,286 @@ __global__ void __launch_bounds__(BLOCK) k_bulk(const __grid_constant__ LatParam
     R rho, ux, uy, uz;
     const R om0[3] = {0, 0, 0};
     relax<R, COLL>(p, k, f, x, y, z, false, 0, 0, 0, 0, 0, om0, rho, ux, uy, uz);
-    store_out<S, P>(p, n, nb, f, s.seed);
+    Rng rng{sr_hash(n, s.seed)};
+    store_out<S, P>(p, n, nb, f, rng);
+}
+
+// ---------------------------------------------------------------- staged bulk
+// The hot loop, staged through shared memory by the bulk-copy (TMA) engine.
+//
+// In the AA pattern a cell reads and writes the same slots: at input parity
+// 0 cell n uses (n, i) for every i; at parity 1 it reads (n + c_j, j) as its
+// input f[opp j] and writes its output f[j] there.  So for a tile of T
+// consecutive cells, plane j's slots form one contiguous range (shifted by
+// c_j at parity 1), and the tile can be updated in place: one
+// cp.async.bulk per plane brings the range into shared memory, every thread
+// overwrites its cell's 19 inputs with its 19 outputs at the same positions,
+// and the ranges go back to HBM with bulk stores (the 16-byte-aligned
+// interior; the few ragged elements at the ends with plain stores).  Cells
+// the kernel skips (faces, walls, solids) keep their slots unchanged.
+//
+// With NX * element size a multiple of 16 bytes and 512-byte aligned planes,
+// a shifted range's misalignment depends only on c_x, so each plane's first
+// cell sits at a compile-time element offset lead in its slot.  Store ranges
+// are clamped to real cells and real slots, so no two blocks write the same
+// slot.  Requires non-periodic x and y; a periodic z wraps only at the z
+// boundaries, where cells load and store their wrapped links directly.
+//
+// Blocks are persistent and double buffered (the next tile's copies are in
+// flight while the current one is collided).  Every mbarrier wait is
+// bounded; on expiry the block records ERR_COPY_WAIT, drains its copies
+// (bounded) and stops.
+// Warp-specialized: warps 0..6 collide (224 threads), warp 7 is the
+// producer that issues the bulk loads and stores.  Per buffer a "full"
+// mbarrier (producer arrival + transaction bytes) and an "empty" mbarrier
+// (one arrival per compute thread) replace block barriers, so compute warps
+// move on to the next tile while the producer writes the last one back.
+constexpr int CWARPS = 7, CTHREADS = CWARPS * 32;
+template <class S> struct Tile { static constexpr uint32_t cells = sizeof(S) == 2 ? 2 * CTHREADS : CTHREADS; };
+template <class S> constexpr uint32_t slot_bytes() { return Tile<S>::cells * (uint32_t)sizeof(S) + 16; }
+template <class S> constexpr uint32_t buf_bytes() { return 19 * slot_bytes<S>() + Tile<S>::cells * 4; }
+template <class S> constexpr uint32_t tma_smem() { return 2 * buf_bytes<S>() + 128; }  // + alignment slack
+
+// element offset of plane j's first tile cell in its shared-memory slot
+template <class S, int P>
+__host__ __device__ __forceinline__ constexpr int lead(int j) {
+    return (P == 0 || j == 0) ? 0 : (CX(j) == 1 ? 1 : (CX(j) == -1 ? (int)(16 / sizeof(S)) - 1 : 0));
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void *ptr) { return (uint32_t)__cvta_generic_to_shared(ptr); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+    for (uint32_t it = 0; it < (1u << 22); it++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_s2g(void *dst, const void *src, uint32_t bytes) {
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_addr(src)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// signed element shift of plane j's slots relative to the cell at parity P
+template <int P>
+__device__ __forceinline__ int64_t plane_shift(int j, int64_t NX, int64_t NXY) {
+    return (P == 0 || j == 0) ? 0 : (int64_t)CX(j) + (int64_t)CY(j) * NX + (int64_t)CZ(j) * NXY;
+}
+
+template <class S, int P>
+__device__ __forceinline__ void tma_load_tile(const LatParams &p, uint8_t *buf, uint64_t *bar, uint32_t n0) {
+    constexpr uint32_t SLOT = slot_bytes<S>();
+    constexpr uint32_t T = Tile<S>::cells;
+    const S *pop = (const S *)p.pop;
+    const int64_t NX = p.NX, NXY = (int64_t)p.NX * p.NY;
+    mbar_expect_tx(bar, 19 * SLOT + T * 4);
+#pragma unroll
+    for (int j = 0; j < 19; j++) {
+        const int64_t e = (int64_t)j * (int64_t)p.NP + n0 + plane_shift<P>(j, NX, NXY) - lead<S, P>(j);
+        bulk_g2s(buf + j * SLOT, pop + e, SLOT, bar);
+    }
+    bulk_g2s(buf + 19 * SLOT, p.flags + n0, T * 4, bar);
+}
+
+// A cell of a periodic-z boundary plane at input parity 1: the links that
+// leave the domain in z wrap to the other side, so those inputs and outputs go
+// straight to HBM; the others use the staged tile like every other cell.
+template <class S, int COLL>
+__device__ __noinline__ void zwrap_cell(const LatParams &p, const StepParams &s, uint8_t *buf, uint32_t c, uint32_t n, uint32_t x,
+                                        uint32_t y, uint32_t z) {
+    using R = typename Pop<S>::real;
+    constexpr uint32_t SLOT = slot_bytes<S>();
+    S *pop = (S *)p.pop;
+    const int zw = z == 0 ? -1 : 1;
+    const Nb nb = make_nb(p, x, y, z);
+    R f[19];
+#pragma unroll
+    for (int i = 0; i < 19; i++) {
+        const int j = i == 0 ? 0 : OPP(i);
+        if (i > 0 && CZ(i) == -zw) f[i] = Pop<S>::ld(pop + (uint64_t)j * p.NP + (uint32_t)((int32_t)n + nb.off(-CX(i), -CY(i), -CZ(i))));
+        else f[i] = Pop<S>::cvt(((const S *)(buf + j * SLOT))[lead<S, 1>(j) + c]);
+    }
+    R rho, ux, uy, uz;
+    const R om0[3] = {0, 0, 0};
+    relax<R, COLL>(p, K<R>(p), f, x, y, z, false, 0, 0, 0, 0, 0, om0, rho, ux, uy, uz);
+    Rng rng{sr_hash(n, s.seed)};
+#pragma unroll
+    for (int i = 0; i < 19; i++) {
+        const S v = Pop<S>::enc(f[i], rng);
+        if (i > 0 && CZ(i) == zw) pop[(uint64_t)i * p.NP + (uint32_t)((int32_t)n + nb.off(CX(i), CY(i), CZ(i)))] = v;
+        else ((S *)(buf + i * SLOT))[lead<S, 1>(i) + c] = v;
+    }
+}
+
+template <class S, int P, int COLL>
+__global__ void __launch_bounds__(BLOCK, sizeof(S) == 8 ? 2 : 3) k_bulk_tma(const __grid_constant__ LatParams p, const __grid_constant__ StepParams s) {
+    using R = typename Pop<S>::real;
+    constexpr uint32_t T = Tile<S>::cells, SLOT = slot_bytes<S>(), BUF = buf_bytes<S>();
+    constexpr int64_t E16 = 16 / sizeof(S);
+    extern __shared__ __align__(128) uint8_t sm_raw[];
+    // realigned with pointer arithmetic so the compiler keeps it a shared-memory pointer
+    uint8_t *sm = sm_raw + ((128u - (smem_addr(sm_raw) & 127u)) & 127u);
+    __shared__ __align__(8) uint64_t full[2], empty[2];
+    __shared__ int64_t tab_sh[19];  // plane shift (elements)
+    __shared__ int tab_lead[19];    // plane lead (elements)
+    const uint32_t ntiles = (p.N + T - 1) / T;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        mbar_init(&full[0], 1);
+        mbar_init(&full[1], 1);
+        mbar_init(&empty[0], CTHREADS);
+        mbar_init(&empty[1], CTHREADS);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (threadIdx.x == 32) {
+#pragma unroll
+        for (int j = 0; j < 19; j++) {
+            tab_sh[j] = plane_shift<P>(j, (int64_t)p.NX, (int64_t)p.NX * p.NY);
+            tab_lead[j] = lead<S, P>(j);
+        }
+    }
+    __syncthreads();
+    S *pop = (S *)p.pop;
+    if (warp == CWARPS) {
+        // ------------------------------------------------ producer warp
+        // iteration it (0 .. K+1 for this block's K tiles): write back tile
+        // it-2 from buffer it&1 once the compute warps released it, then load
+        // tile it into the same buffer
+        const int64_t N = p.N;
+        const uint32_t G = gridDim.x;
+        const uint32_t K = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / G + 1 : 0;
+        uint32_t it = 0;
+        bool alive = true;
+        for (; it < K + 2; ++it) {
+            const int b = it & 1;
+            if (it >= 2) {
+                if (!mbar_wait_bounded(&empty[b], ((it - 2) >> 1) & 1)) { alive = false; break; }
+                if (lane < 19) {
+                    // plane j's slots of the tile's cells back to HBM: cells
+                    // and slots clamped to [0, N); the 16-byte-aligned interior
+                    // with one bulk store, the ragged ends with plain stores
+                    const int j = lane;
+                    const uint32_t n0 = (blockIdx.x + (it - 2) * G) * T;
+                    const int64_t sh = tab_sh[j];
+                    const int64_t lo = max((int64_t)n0, -sh);
+                    int64_t hi = min(min((int64_t)n0 + (int64_t)T, N), N - sh);
+                    if (hi < lo) hi = lo;
+                    int64_t a = ((lo + sh + E16 - 1) & ~(E16 - 1)) - sh;  // slots are >= 0 here
+                    int64_t bb = ((hi + sh) & ~(E16 - 1)) - sh;
+                    if (bb < a) { a = hi; bb = hi; }
+                    S *dst = pop + (int64_t)j * (int64_t)p.NP + sh;
+                    const S *src = (const S *)(sm + b * BUF + j * SLOT) + tab_lead[j] - (int64_t)n0;
+                    if (bb > a) bulk_s2g(dst + a, src + a, (uint32_t)((bb - a) * (int64_t)sizeof(S)));
+                    bulk_commit();
+                    for (int64_t m = lo; m < min(a, hi); m++) dst[m] = src[m];
+                    for (int64_t m = max(bb, lo); m < hi; m++) dst[m] = src[m];
+                    bulk_wait_read_all();
+                }
+                __syncwarp();
+            }
+            if (it < K && lane == 0) {
+                fence_async_smem();
+                tma_load_tile<S, P>(p, sm + b * BUF, &full[b], (blockIdx.x + it * G) * T);
+            }
+        }
+        if (!alive && lane == 0) {
+            atomicOr(p.err, ERR_COPY_WAIT);
+            // drain the loads still in flight (the last one into each buffer)
+            for (int bq = 0; bq < 2; bq++) {
+                int last = -1;
+                for (uint32_t q = 0; q < min(it, K); q++)
+                    if ((int)(q & 1) == bq) last = (int)q;
+                if (last >= 0) mbar_wait_bounded(&full[bq], ((uint32_t)last >> 1) & 1);
+            }
+        }
+        if (lane < 19) bulk_wait_all();
+        return;
+    }
+    // ---------------------------------------------------- compute warps
+    const Consts<R> &k = K<R>(p);
+    const bool zper = p.per[2] != 0;
+    uint32_t it = 0;
+    for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
+        const int b = it & 1;
+        if (!mbar_wait_bounded(&full[b], (it >> 1) & 1)) {
+            atomicOr(p.err, ERR_COPY_WAIT);
+            return;
+        }
+        uint8_t *buf = sm + b * BUF;
+        const uint32_t *fl = (const uint32_t *)(buf + 19 * SLOT);
+        const uint32_t n0 = t * T;
+#pragma unroll 1
+        for (uint32_t c = threadIdx.x; c < T; c += CTHREADS) {
+            const uint32_t n = n0 + c;
+            if (n >= p.N) break;
+            if (fl[c] != 0u) continue;
+            uint32_t x, y, z;
+            coords(p, n, x, y, z);
+            if (P == 1 && zper && (z == 0 || z == p.NZ - 1)) {
+                zwrap_cell<S, COLL>(p, s, buf, c, n, x, y, z);
+                continue;
+            }
+            // FP16 values stay in storage units (x 32768) through the collision
+            constexpr int SC = std::is_same<S, __half>::value ? 32768 : 1;
+            R f[19];
+#pragma unroll
+            for (int i = 0; i < 19; i++) {
+                const int j = (P == 0 || i == 0) ? i : OPP(i);  // plane holding input f[i]
+                const S v = ((const S *)(buf + j * SLOT))[lead<S, P>(j) + c];
+                if constexpr (SC != 1) f[i] = __half2float(v);
+                else f[i] = Pop<S>::cvt(v);
+            }
+            R rho, ux, uy, uz;
+            const R om0[3] = {0, 0, 0};
+            relax<R, COLL, SC>(p, k, f, x, y, z, false, 0, 0, 0, 0, 0, om0, rho, ux, uy, uz);
+            Rng rng{sr_hash(n, s.seed)};
+            S out[19];
+            if constexpr (SC != 1) {
+                // stochastic rounding noise per value, then one packed
+                // round-toward-zero conversion per pair of outputs
+#pragma unroll
+                for (int i = 0; i < 18; i += 2) {
+                    const uint32_t h2 = cvt_rz_f16x2(sr_noise13(f[i + 1], rng), sr_noise13(f[i], rng));
+                    out[i] = __ushort_as_half((unsigned short)(h2 & 0xffffu));
+                    out[i + 1] = __ushort_as_half((unsigned short)(h2 >> 16));
+                }
+                out[18] = __float2half_rz(sr_noise13(f[18], rng));
+            } else {
+#pragma unroll
+                for (int i = 0; i < 19; i++) out[i] = Pop<S>::enc(f[i], rng);
+            }
+#pragma unroll
+            for (int i = 0; i < 19; i++) {
+                const int j = (P == 0) ? OPP(i) : i;  // plane receiving output f[i]
+                ((S *)(buf + j * SLOT))[lead<S, P>(j) + c] = out[i];
+            }
+        }
+        fence_async_smem();  // this thread's shared-memory writes, before the bulk stores read them
+        mbar_arrive(&empty[b]);
+    }
 }
 
 // ---------------------------------------------------------------- walls
@@ -238,7 +603,8 @@ __global__ void __launch_bounds__(BLOCK) k_walls(const __grid_constant__ LatPara
                 for (int a = 0; a < 3; a++) { Fo[a] += Rec<R>::ft(p, r, a); To[a] += Rec<R>::ft(p, r, 3 + a); }
             }
             for (int a = 0; a < 3; a++) { Rec<R>::set_ft(p, r, a, Fo[a]); Rec<R>::set_ft(p, r, 3 + a, To[a]); }
-            store_out<S, P>(p, cell, nb, f, s.seed);
+            Rng rng{sr_hash(cell, s.seed)};
+            store_out<S, P>(p, cell, nb, f, rng);
         } else {
             for (int a = 0; a < 3; a++) { Fo[a] = Rec<R>::ft(p, r, a); To[a] = Rec<R>::ft(p, r, 3 + a); }
         }
@@ -368,7 +734,8 @@ __global__ void __launch_bounds__(BLOCK) k_faces(const __grid_constant__ LatPara
         for (int i = 0; i < 19; i++) f[i] = feq_i<R>(i, rho1, rho, ux, uy, uz, usq) + fneq_i<R>(i, pi, tr);
     }
     const Nb nbb = make_nb(p, x, y, z);
-    store_prev_out<S, Q>(p, b, x, y, z, nbb, f, s.seed);
+    Rng rng{sr_hash(b, s.seed)};
+    store_prev_out<S, Q>(p, b, x, y, z, nbb, f, rng);
 }
 
 // ---------------------------------------------------------------- init
@@ -381,9 +748,9 @@ __global__ void __launch_bounds__(BLOCK) k_init(const __grid_constant__ LatParam
     if (n >= p.N) return;
     S *pop = (S *)p.pop;
     const R usq = (R)1.5 * (k.u_init[0] * k.u_init[0] + k.u_init[1] * k.u_init[1] + k.u_init[2] * k.u_init[2]);
+    Rng rng{sr_hash(n, 0u)};
 #pragma unroll
-    for (int i = 0; i < 19; i++)
-        Pop<S>::st(pop + (size_t)i * p.N + n, feq_i<R>(i, (R)0, (R)1, k.u_init[0], k.u_init[1], k.u_init[2], usq), n * 19u + (uint32_t)i, 0u);
+    for (int i = 0; i < 19; i++) pop[(uint64_t)i * p.NP + n] = Pop<S>::enc(feq_i<R>(i, (R)0, (R)1, k.u_init[0], k.u_init[1], k.u_init[2], usq), rng);
 }
 
 // ---------------------------------------------------------------- dump
@@ -502,8 +869,9 @@ __global__ void __launch_bounds__(BLOCK) k_sample_slices(const __grid_constant__
 }
 
 // ---------------------------------------------------------------- mass
-// FP64 sum of rho over fluid cells (wall cells from their records) and a
-// count of non-finite densities.
+// FP64 sum of rho over fluid cells (wall cells included) from the
+// post-collision populations of the last step, and a count of non-finite
+// densities.
 template <class S, int Q>
 __global__ void __launch_bounds__(BLOCK) k_mass(const __grid_constant__ LatParams p, double *mass, unsigned long long *bad) {
     using R = typename Pop<S>::real;
@@ -513,21 +881,15 @@ __global__ void __launch_bounds__(BLOCK) k_mass(const __grid_constant__ LatParam
     if (n < p.N) {
         const uint32_t fg = p.flags[n];
         if ((fg & 3u) == 0u) {
-            const uint32_t rec = fg >> 2;
-            double rho;
-            if (rec) {
-                rho = (double)Rec<R>::macro(p, rec - 1, 0);
-            } else {
-                uint32_t x, y, z;
-                coords(p, n, x, y, z);
-                const Nb nb = make_nb(p, x, y, z);
-                R f[19];
-                load_prev_out<S, Q>(p, n, nb, f);
-                double s = 0;
+            uint32_t x, y, z;
+            coords(p, n, x, y, z);
+            const Nb nb = make_nb(p, x, y, z);
+            R f[19];
+            load_prev_out<S, Q>(p, n, nb, f);
+            double s = 0;
 #pragma unroll
-                for (int i = 0; i < 19; i++) s += (double)f[i];
-                rho = 1.0 + s;
-            }
+            for (int i = 0; i < 19; i++) s += (double)f[i];
+            const double rho = 1.0 + s;
             if (isfinite(rho)) v = rho; else nb_bad = 1;
         }
     }
@@ -542,6 +904,31 @@ __global__ void __launch_bounds__(BLOCK) k_mass(const __grid_constant__ LatParam
 // ---------------------------------------------------------------- launchers
 static inline unsigned blocks_for(uint64_t n) { return (unsigned)((n + BLOCK - 1) / BLOCK); }
 
+static int num_sms() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 1;
+    }
+    return n;
+}
+
+// persistent grid of the staged kernel: resident blocks per SM x SMs
+template <class S, int P, int COLL>
+static unsigned tma_grid() {
+    static unsigned g = 0;
+    if (!g) {
+        auto kern = k_bulk_tma<S, P, COLL>;
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem<S>());
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BLOCK, tma_smem<S>());
+        g = (unsigned)(std::max(per_sm, 1) * num_sms());
+    }
+    return g;
+}
+
 template <class S, int P, int COLL>
 static cudaError_t step_t(const LatParams &p, const StepParams &s, cudaStream_t st, cudaEvent_t *ev) {
     if (ev) cudaEventRecord(ev[0], st);
@@ -549,7 +936,12 @@ static cudaError_t step_t(const LatParams &p, const StepParams &s, cudaStream_t 
     if (ev) cudaEventRecord(ev[1], st);
     if (p.nrec) k_walls<S, P, COLL><<<blocks_for(p.nrec), BLOCK, 0, st>>>(p, s);
     if (ev) cudaEventRecord(ev[2], st);
-    k_bulk<S, P, COLL><<<blocks_for(p.N), BLOCK, 0, st>>>(p, s);
+    if (p.tma) {
+        const unsigned ntiles = (unsigned)((p.N + Tile<S>::cells - 1) / Tile<S>::cells);
+        k_bulk_tma<S, P, COLL><<<std::min(ntiles, tma_grid<S, P, COLL>()), BLOCK, tma_smem<S>(), st>>>(p, s);
+    } else {
+        k_bulk<S, P, COLL><<<blocks_for(p.N), BLOCK, 0, st>>>(p, s);
+    }
     if (ev) cudaEventRecord(ev[3], st);
     return cudaGetLastError();
 }

@@ -10,6 +10,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <stdexcept>
 #include <string>
@@ -83,6 +84,8 @@ struct lbm_lattice {
     bool prof = false;
     std::vector<cudaEvent_t> prof_ev;
     uint64_t prof_steps = 0;
+    uint64_t pop_bytes = 0;
+    uint32_t *err_host = nullptr;  // pinned
 
     void *dalloc(size_t bytes) {
         void *p = nullptr;
@@ -95,6 +98,7 @@ struct lbm_lattice {
         if (stream) cudaStreamSynchronize(stream);
         for (void *p : allocs) cudaFree(p);
         if (hist_host) cudaFreeHost(hist_host);
+        if (err_host) cudaFreeHost(err_host);
         if (ev) cudaEventDestroy(ev);
         for (cudaEvent_t e : prof_ev) cudaEventDestroy(e);
         if (stream) cudaStreamDestroy(stream);
@@ -112,6 +116,15 @@ struct lbm_lattice {
         }
     }
     int parity() const { return (int)(steps_done % 2); }
+    void check_device_errors() {
+        if (err_host && *err_host) {
+            const uint32_t e = *err_host;
+            *err_host = 0;
+            cudaMemsetAsync(lp.err, 0, 4, stream);
+            if (e & lbm::ERR_COPY_WAIT) throw LbmError(LBM_ERR_TIMEOUT, "a bulk-copy wait in the step kernel passed its iteration limit");
+            throw LbmError(LBM_ERR_CUDA, "device error bits " + std::to_string(e));
+        }
+    }
 };
 
 namespace {
@@ -146,6 +159,17 @@ void fill_consts(lbm::Consts<R> &k, const lbm_setup &st) {
         k.u_init[a] = (R)st.u_init[a];
         k.grav[a] = (R)st.body_force[a];
         k.center[a] = (R)st.center[a];
+        k.sp_lo_inv[a] = st.sponge[2 * a] ? (R)(1.0 / st.sponge[2 * a]) : (R)0;
+        k.sp_hi_inv[a] = st.sponge[2 * a + 1] ? (R)(1.0 / st.sponge[2 * a + 1]) : (R)0;
+    }
+    const double usq = 1.5 * (st.u_inf[0] * st.u_inf[0] + st.u_inf[1] * st.u_inf[1] + st.u_inf[2] * st.u_inf[2]);
+    k.ft_rest = (R)(-(1.0 / 3.0) * usq);
+    for (int kk = 0; kk < 9; kk++) {
+        const int i = 2 * kk + 1;
+        const double w = kk < 3 ? 1.0 / 18.0 : 1.0 / 36.0;
+        const double cu = lbm::CX(i) * st.u_inf[0] + lbm::CY(i) * st.u_inf[1] + lbm::CZ(i) * st.u_inf[2];
+        k.ft_even[kk] = (R)(w * (4.5 * cu * cu - usq));
+        k.ft_odd[kk] = (R)(w * 3.0 * cu);
     }
 }
 
@@ -297,10 +321,19 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     ck(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     ck(cudaEventCreateWithFlags(&h->ev, cudaEventDisableTiming), "cudaEventCreate");
     ck(cudaMallocHost((void **)&h->hist_host, KMAX * 8 * sizeof(double)), "cudaMallocHost");
+    ck(cudaMallocHost((void **)&h->err_host, 16), "cudaMallocHost");
     lbm::LatParams &p = h->lp;
     const size_t sb = storage_bytes(st.storage);
-    p.pop = h->dalloc(19 * N * sb);
-    p.flags = (uint32_t *)h->dalloc(N * 4);
+    // planes padded to 256 cells; a guard after the last plane covers the
+    // shifted tile ranges the staged kernel fetches (largest offset NX*NY+NX+1)
+    const uint64_t NP = (N + lbm::PLANE_ALIGN - 1) / lbm::PLANE_ALIGN * lbm::PLANE_ALIGN;
+    const uint64_t guard = (2048 + NX * NY + NX + 64 + lbm::PLANE_ALIGN - 1) / lbm::PLANE_ALIGN * lbm::PLANE_ALIGN;
+    h->pop_bytes = (19 * NP + guard) * sb;
+    p.pop = h->dalloc(h->pop_bytes);
+    p.NP = NP;
+    const uint64_t NFL = (N + 1023) / 1024 * 1024 + 1024;  // flags padded past the last tile
+    p.flags = (uint32_t *)h->dalloc(NFL * 4);
+    p.err = (uint32_t *)h->dalloc(16);
     p.recs = (uint32_t *)h->dalloc(nrec * lbm::RS * 4);
     p.recd = st.storage == LBM_STORAGE_FP64 ? (double *)h->dalloc(nrec * lbm::RD * 8) : nullptr;
     p.faces = (uint32_t *)h->dalloc(faces.size() * 4);
@@ -315,6 +348,12 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     h->verts = (float *)h->dalloc(std::max<size_t>(vbuf.size(), 8) * 4);
     h->slicedef = (int32_t *)h->dalloc(sd.size() * 4);
     p.NX = (uint32_t)NX; p.NY = (uint32_t)NY; p.NZ = (uint32_t)NZ; p.N = (uint32_t)N;
+    p.div_nx.init((uint32_t)NX);
+    p.div_nxy.init((uint32_t)(NX * NY));
+    // the staged bulk kernel needs x-rows that keep 16-byte alignment and
+    // non-periodic x and y (its in-place tiles own their slots only then)
+    const char *no_tma = std::getenv("SIMLAB_LBM_NO_TMA");
+    p.tma = (NX * sb) % 16 == 0 && !per[0] && !per[1] && !(no_tma && no_tma[0] == '1');
     p.nrec = (uint32_t)nrec; p.nface = (uint32_t)faces.size();
     for (int a = 0; a < 3; a++) p.per[a] = per[a];
     p.abs_u = st.absorb_velocity != 0;
@@ -322,13 +361,19 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     p.wall_model = st.wall_model != 0;
     p.forcing = st.body_force[0] != 0.0 || st.body_force[1] != 0.0 || st.body_force[2] != 0.0;
     p.sponge_on = 0;
-    for (int f = 0; f < 6; f++) p.sponge_on |= st.sponge[f] > 0;
+    for (int f = 0; f < 6; f++) {
+        p.sponge_on |= st.sponge[f] > 0;
+        p.sp_w[f] = st.sponge[f];
+    }
     p.les_on = st.smagorinsky != 0.0;
     p.moving = 0;
     fill_consts<float>(p.kf, st);
     fill_consts<double>(p.kd, st);
 
     cudaStream_t s = h->stream;
+    ck(cudaMemsetAsync(p.pop, 0, h->pop_bytes, s), "memset");
+    ck(cudaMemsetAsync(p.flags, 0, NFL * 4, s), "memset");
+    ck(cudaMemsetAsync(p.err, 0, 16, s), "memset");
     ck(cudaMemcpyAsync(p.flags, flags.data(), N * 4, cudaMemcpyHostToDevice, s), "upload flags");
     if (nrec) ck(cudaMemcpyAsync(p.recs, words.data(), words.size() * 4, cudaMemcpyHostToDevice, s), "upload records");
     if (!wordsd.empty()) ck(cudaMemcpyAsync(p.recd, wordsd.data(), wordsd.size() * 8, cudaMemcpyHostToDevice, s), "upload records");
@@ -346,8 +391,8 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     h->wait();  // host vectors go out of scope after this
 }
 
+// steps == nullptr: n still steps (StepIn::still(false))
 void run_impl(lbm_lattice *h, const lbm_step_in *steps, uint64_t n, double *forces_out, bool readback) {
-    if (n && !steps) throw LbmError(LBM_ERR_INVALID, "steps is null");
     lbm::LatParams &p = h->lp;
     lbm_step_in still{};
     for (int a = 0; a < 3; a++) { still.rot[a][a] = 1.0; still.rot_prev[a][a] = 1.0; }
@@ -378,7 +423,9 @@ void run_impl(lbm_lattice *h, const lbm_step_in *steps, uint64_t n, double *forc
         }
         if (readback) {
             ck(cudaMemcpyAsync(h->hist_host, p.hist, len * 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "history readback");
+            ck(cudaMemcpyAsync(h->err_host, p.err, 4, cudaMemcpyDeviceToHost, h->stream), "error readback");
             h->wait();
+            h->check_device_errors();
             if (forces_out)
                 for (uint32_t k = 0; k < len; k++)
                     for (int j = 0; j < 6; j++) forces_out[(c0 + k) * 6 + j] = h->hist_host[k * 8 + j];
@@ -432,6 +479,7 @@ void lbm_destroy(lbm_lattice *h) { delete h; }
 
 int lbm_run(lbm_lattice *h, const lbm_step_in *steps, uint64_t n, double *forces_out) {
     if (!h) return LBM_ERR_INVALID;
+    if (n && !steps) return fail(h, LbmError(LBM_ERR_INVALID, "steps is null"));
     return guard(h, [&] { run_impl(h, steps, n, forces_out, true); });
 }
 
@@ -578,8 +626,7 @@ static const uint64_t STATE_MAGIC = 0x4c424d5354415431ull;
 
 int lbm_state_size(const lbm_lattice *h, uint64_t *bytes) {
     if (!h || !bytes) return LBM_ERR_INVALID;
-    const uint64_t N = h->lp.N;
-    *bytes = sizeof(StateHeader) + 19 * N * storage_bytes(h->setup.storage) + (uint64_t)h->nrec * lbm::RS * 4 +
+    *bytes = sizeof(StateHeader) + 19 * h->lp.NP * storage_bytes(h->setup.storage) + (uint64_t)h->nrec * lbm::RS * 4 +
              (h->lp.recd ? (uint64_t)h->nrec * lbm::RD * 8 : 0);
     return LBM_OK;
 }
@@ -594,7 +641,7 @@ int lbm_save_state(lbm_lattice *h, void *buf, uint64_t bytes) {
         char *o = (char *)buf;
         std::memcpy(o, &hd, sizeof hd);
         o += sizeof hd;
-        const uint64_t pb = 19ull * h->lp.N * storage_bytes(h->setup.storage);
+        const uint64_t pb = 19ull * h->lp.NP * storage_bytes(h->setup.storage);
         ck(cudaMemcpyAsync(o, h->lp.pop, pb, cudaMemcpyDeviceToHost, h->stream), "state readback");
         o += pb;
         if (h->nrec) ck(cudaMemcpyAsync(o, h->lp.recs, (size_t)h->nrec * lbm::RS * 4, cudaMemcpyDeviceToHost, h->stream), "state readback");
@@ -615,7 +662,7 @@ int lbm_load_state(lbm_lattice *h, const void *buf, uint64_t bytes) {
         if (hd.magic != STATE_MAGIC || hd.cells != h->lp.N || hd.nrec != h->nrec || hd.storage != h->setup.storage)
             throw LbmError(LBM_ERR_INVALID, "state does not belong to this lattice");
         const char *o = (const char *)buf + sizeof hd;
-        const uint64_t pb = 19ull * h->lp.N * storage_bytes(h->setup.storage);
+        const uint64_t pb = 19ull * h->lp.NP * storage_bytes(h->setup.storage);
         ck(cudaMemcpyAsync(h->lp.pop, o, pb, cudaMemcpyHostToDevice, h->stream), "state upload");
         o += pb;
         if (h->nrec) ck(cudaMemcpyAsync(h->lp.recs, o, (size_t)h->nrec * lbm::RS * 4, cudaMemcpyHostToDevice, h->stream), "state upload");

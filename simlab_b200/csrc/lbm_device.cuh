@@ -1,9 +1,17 @@
 // Device-side building blocks of the D3Q19 time step: the velocity set,
 // population storage formats (FP32 / FP64 / FP16 / BF16 deviations from the
-// weights), stochastic rounding, launch parameters and record access.
+// weights), stochastic rounding, launch parameters, record access and the
+// AA-pattern access functions.
 //
 // Reference semantics: crates/cfd/src/shader.rs (velocity set 22-60, record
-// layout 62-69, storage 147-162, stochastic rounding 507-517).
+// layout 62-69, storage 147-162, stochastic rounding 507-517, AA access
+// 254-339).
+//
+// HBM layout: the 19 population planes are stored slot-major like the
+// reference (direction d of cell n at d * NP + n), with the plane stride NP
+// rounded up to 256 cells so every plane starts 512-byte aligned, and guard
+// zones before the first and after the last plane so the shifted ranges the
+// bulk copies fetch for a tile never leave the allocation.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -15,7 +23,8 @@ namespace lbm {
 
 // ------------------------------------------------------------ velocity set
 // D3Q19 in the reference's order: rest, +-x, +-y, +-z, then the 12 edges
-// (shader.rs:22-42); opposite directions are neighbours (shader.rs:44-52).
+// (shader.rs:22-42); opposite directions are neighbours (shader.rs:44-52), so
+// the 9 pairs (2k+1, 2k+2) each hold a velocity and its opposite.
 __host__ __device__ __forceinline__ constexpr int CX(int i) {
     return (i == 1 || i == 7 || i == 9 || i == 13 || i == 15) ? 1 : ((i == 2 || i == 8 || i == 10 || i == 14 || i == 16) ? -1 : 0);
 }
@@ -40,16 +49,47 @@ constexpr uint32_t RS = 40, R_MASK = 0, R_CELL = 1, R_Q = 2, R_FPOST = 11, R_MAC
 constexpr uint32_t RD = 28, RD_FPOST = 0, RD_MACRO = 18, RD_FT = 22;
 
 constexpr int BLOCK = 256;
+constexpr uint32_t PLANE_ALIGN = 256;  // cells
+
+// error bits set by kernels (read by the host after each chunk)
+constexpr uint32_t ERR_COPY_WAIT = 1u;  // a bulk-copy wait passed its iteration limit
+
+// ------------------------------------------------------------ fast division
+// Unsigned 32-bit division by a run-time constant with a multiply-high
+// (Granlund & Montgomery 1994, round-up multiplier with a 33-bit add):
+// q = (umulhi(n, m) + n) >> s, exact for every 32-bit n.
+struct FastDiv {
+    uint32_t d, m, s;
+    __host__ void init(uint32_t div) {
+        d = div;
+        s = 0;
+        while ((1ull << s) < div) s++;
+        m = (uint32_t)((((1ull << s) - div) << 32) / div + 1);
+        if (div == 1) { m = 0; s = 0; }
+    }
+    __host__ __device__ __forceinline__ uint32_t div(uint32_t n) const {
+#ifdef __CUDA_ARCH__
+        const uint32_t hi = __umulhi(n, m);
+#else
+        const uint32_t hi = (uint32_t)(((uint64_t)n * m) >> 32);
+#endif
+        return (uint32_t)(((uint64_t)hi + n) >> s);
+    }
+};
 
 // ------------------------------------------------------------ launch params
 template <class R>
 struct Consts {
     R tau0, smag2, sponge_tau, sigma;
     R sp_lo[3], sp_hi[3], u_inf[3], u_init[3], grav[3], center[3];
+    R sp_lo_inv[3], sp_hi_inv[3];  // reciprocal sponge widths (0 where no sponge)
+    // shifted equilibrium at rest density and u_inf: the absorbing target when
+    // absorb_velocity (rest, then the even and odd parts of the 9 pairs)
+    R ft_rest, ft_even[9], ft_odd[9];
 };
 
 struct LatParams {
-    void *pop;                 // 19 * N stored populations, slot-major (d * N + cell)
+    void *pop;                 // plane 0 of 19 planes, plane stride NP cells
     uint32_t *flags;           // N words: 0 fluid, 1 solid, 2/3 face, (rec+1)<<2 wall cell
     uint32_t *recs;            // nrec * RS words
     double *recd;              // FP64 engine: nrec * RD doubles (else null)
@@ -59,10 +99,15 @@ struct LatParams {
     uint32_t *ticket;          // last-block counter of the force reduction
     double *hist;              // per step slot: 8 doubles (F, T)
     float4 *dump;              // macros() output
+    uint32_t *err;             // error bits (ERR_*)
+    uint64_t NP;               // plane stride (cells)
     uint32_t NX, NY, NZ, N;
+    FastDiv div_nx, div_nxy;
     uint32_t nrec, nface;
     int per[3];
     int abs_u, total_p, wall_model, forcing, sponge_on, les_on, moving;
+    uint32_t sp_w[6];          // sponge widths in cells, -x,+x,-y,+y,-z,+z
+    int tma;                   // the staged bulk kernel applies (NX * element size % 16 == 0)
     Consts<float> kf;
     Consts<double> kd;
 };
@@ -80,56 +125,74 @@ template <> __device__ __forceinline__ const Consts<float> &K<float>(const LatPa
 template <> __device__ __forceinline__ const Consts<double> &K<double>(const LatParams &p) { return p.kd; }
 
 // ------------------------------------------------------------ rounding
-// shader.rs:510-517: noise uniform in [-1/2, 1/2) of one unit in the last
-// place, from an integer hash of the slot key and the step seed.
-__device__ __forceinline__ uint32_t sr_hash(uint32_t key, uint32_t seed) {
+// Stochastic rounding (shader.rs:507-517): a value is rounded up with
+// probability equal to its fractional part in units of the target format's
+// last place, so slow changes below half an ulp still accumulate.  The
+// reference adds uniform noise in [-1/2, 1/2) ulp from an integer hash of
+// (cell * 19 + slot, step seed) and rounds to nearest.  Here the same
+// distribution comes from adding uniform random bits below the kept mantissa
+// and truncating: one hash per cell (the reference's mixer keyed by the cell
+// and the step seed) seeds a 32-bit linear congruential sequence (Numerical
+// Recipes constants) whose top bits serve the cell's stores in turn.
+__host__ __device__ __forceinline__ uint32_t sr_hash(uint32_t key, uint32_t seed) {
     uint32_t h = (key * 0x9E3779B1u) ^ (seed * 0x85EBCA77u + 0x632BE5ABu);
     h ^= h >> 16; h *= 0x7feb352du; h ^= h >> 15; h *= 0x846ca68bu; h ^= h >> 16;
     return h;
 }
-__device__ __forceinline__ float pow2i(int e) { return __uint_as_float((uint32_t)(e + 127) << 23); }  // 2^e, normal e
+struct Rng {
+    uint32_t s;
+    __device__ __forceinline__ uint32_t next() {
+        s = s * 1664525u + 1013904223u;
+        return s;
+    }
+};
 
-__device__ __forceinline__ float sround16(float x, uint32_t key, uint32_t seed) {
-    float r = (float)(sr_hash(key, seed) >> 8) * (1.0f / 16777216.0f) - 0.5f;
-    int e = (int)((__float_as_uint(x) >> 23) & 0xffu) - 127;
-    float ulp = pow2i(max(e, -14) - 10);
-    float v = __fadd_rn(x, __fmul_rn(r, ulp));
-    return fminf(fmaxf(v, -65000.0f), 65000.0f);
+// FP16 stores (f - w) * 32768; 13 random bits below binary16's 10-bit
+// mantissa, then round toward zero (which also saturates at the largest
+// finite half instead of overflowing).
+__device__ __forceinline__ float sr_f16_pre(float v, Rng &r) {
+    return __uint_as_float(__float_as_uint(v * 32768.0f) + (r.next() >> 19));
 }
-__device__ __forceinline__ float sround_bf16(float x, uint32_t key, uint32_t seed) {
-    float r = (float)(sr_hash(key, seed) >> 8) * (1.0f / 16777216.0f) - 0.5f;
-    int e = (int)((__float_as_uint(x) >> 23) & 0xffu) - 127;
-    float ulp = pow2i(max(e, -126) - 7);
-    return __fadd_rn(x, __fmul_rn(r, ulp));
+__device__ __forceinline__ __half sr_f16(float v, Rng &r) { return __float2half_rz(sr_f16_pre(v, r)); }
+// noise only, for values already in storage units
+__device__ __forceinline__ float sr_noise13(float v, Rng &r) { return __uint_as_float(__float_as_uint(v) + (r.next() >> 19)); }
+// two values at once: {hi, lo} = rz(a), rz(b)
+__device__ __forceinline__ uint32_t cvt_rz_f16x2(float a, float b) {
+    uint32_t d;
+    asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(a), "f"(b));
+    return d;
+}
+// BF16 stores (f - w) as is; 16 random bits below bfloat16's mantissa, then truncate.
+__device__ __forceinline__ __nv_bfloat16 sr_bf16(float v, Rng &r) {
+    const uint32_t b = __float_as_uint(v) + (r.next() >> 16);
+    return __ushort_as_bfloat16((unsigned short)(b >> 16));
 }
 
 // ------------------------------------------------------------ storage
-// Every format stores f_i - w_i.  FP16 multiplies by 32768 first
-// (shader.rs:73, 153-162); BF16 keeps the value as is.
 template <class S> struct Pop;
 template <> struct Pop<float> {
     using real = float;
+    static __device__ __forceinline__ float cvt(float v) { return v; }
     static __device__ __forceinline__ float ld(const float *p) { return *p; }
-    static __device__ __forceinline__ void st(float *p, float v, uint32_t, uint32_t) { *p = v; }
+    static __device__ __forceinline__ float enc(float v, Rng &) { return v; }
 };
 template <> struct Pop<double> {
     using real = double;
+    static __device__ __forceinline__ double cvt(double v) { return v; }
     static __device__ __forceinline__ double ld(const double *p) { return *p; }
-    static __device__ __forceinline__ void st(double *p, double v, uint32_t, uint32_t) { *p = v; }
+    static __device__ __forceinline__ double enc(double v, Rng &) { return v; }
 };
 template <> struct Pop<__half> {
     using real = float;
-    static __device__ __forceinline__ float ld(const __half *p) { return __half2float(*p) * (1.0f / 32768.0f); }
-    static __device__ __forceinline__ void st(__half *p, float v, uint32_t key, uint32_t seed) {
-        *p = __float2half_rn(sround16(v * 32768.0f, key, seed));
-    }
+    static __device__ __forceinline__ float cvt(__half v) { return __half2float(v) * (1.0f / 32768.0f); }
+    static __device__ __forceinline__ float ld(const __half *p) { return cvt(*p); }
+    static __device__ __forceinline__ __half enc(float v, Rng &r) { return sr_f16(v, r); }
 };
 template <> struct Pop<__nv_bfloat16> {
     using real = float;
-    static __device__ __forceinline__ float ld(const __nv_bfloat16 *p) { return __bfloat162float(*p); }
-    static __device__ __forceinline__ void st(__nv_bfloat16 *p, float v, uint32_t key, uint32_t seed) {
-        *p = __float2bfloat16_rn(sround_bf16(v, key, seed));
-    }
+    static __device__ __forceinline__ float cvt(__nv_bfloat16 v) { return __bfloat162float(v); }
+    static __device__ __forceinline__ float ld(const __nv_bfloat16 *p) { return cvt(*p); }
+    static __device__ __forceinline__ __nv_bfloat16 enc(float v, Rng &r) { return sr_bf16(v, r); }
 };
 
 // ------------------------------------------------------------ records
@@ -188,10 +251,9 @@ __device__ __forceinline__ Nb make_nb(const LatParams &p, uint32_t x, uint32_t y
 }
 
 __device__ __forceinline__ void coords(const LatParams &p, uint32_t n, uint32_t &x, uint32_t &y, uint32_t &z) {
-    uint32_t nxy = p.NX * p.NY;
-    z = n / nxy;
-    uint32_t r = n - z * nxy;
-    y = r / p.NX;
+    z = p.div_nxy.div(n);
+    const uint32_t r = n - z * (p.NX * p.NY);
+    y = p.div_nx.div(r);
     x = r - y * p.NX;
 }
 
@@ -203,23 +265,22 @@ __device__ __forceinline__ void coords(const LatParams &p, uint32_t n, uint32_t 
 template <class S, int P>
 __device__ __forceinline__ void load_in(const LatParams &p, uint32_t n, const Nb &nb, typename Pop<S>::real *f) {
     const S *pop = (const S *)p.pop;
-    const size_t N = p.N;
+    const uint64_t NP = p.NP;
 #pragma unroll
     for (int i = 0; i < 19; i++) {
-        if (P == 0 || i == 0) f[i] = Pop<S>::ld(pop + (size_t)i * N + n);
-        else f[i] = Pop<S>::ld(pop + (size_t)OPP(i) * N + (uint32_t)((int32_t)n + nb.off(-CX(i), -CY(i), -CZ(i))));
+        if (P == 0 || i == 0) f[i] = Pop<S>::ld(pop + (uint64_t)i * NP + n);
+        else f[i] = Pop<S>::ld(pop + (uint64_t)OPP(i) * NP + (uint32_t)((int32_t)n + nb.off(-CX(i), -CY(i), -CZ(i))));
     }
 }
 
 template <class S, int P>
-__device__ __forceinline__ void store_out(const LatParams &p, uint32_t n, const Nb &nb, const typename Pop<S>::real *f, uint32_t seed) {
+__device__ __forceinline__ void store_out(const LatParams &p, uint32_t n, const Nb &nb, const typename Pop<S>::real *f, Rng &rng) {
     S *pop = (S *)p.pop;
-    const size_t N = p.N;
-    const uint32_t key0 = n * 19u;
+    const uint64_t NP = p.NP;
 #pragma unroll
     for (int i = 0; i < 19; i++) {
-        if (P == 0 || i == 0) Pop<S>::st(pop + (size_t)OPP(i) * N + n, f[i], key0 + (uint32_t)OPP(i), seed);
-        else Pop<S>::st(pop + (size_t)i * N + (uint32_t)((int32_t)n + nb.off(CX(i), CY(i), CZ(i))), f[i], key0 + (uint32_t)i, seed);
+        if (P == 0 || i == 0) pop[(uint64_t)OPP(i) * NP + n] = Pop<S>::enc(f[i], rng);
+        else pop[(uint64_t)i * NP + (uint32_t)((int32_t)n + nb.off(CX(i), CY(i), CZ(i)))] = Pop<S>::enc(f[i], rng);
     }
 }
 
@@ -228,11 +289,11 @@ __device__ __forceinline__ void store_out(const LatParams &p, uint32_t n, const 
 template <class S, int Q>
 __device__ __forceinline__ void load_prev_out(const LatParams &p, uint32_t n, const Nb &nb, typename Pop<S>::real *f) {
     const S *pop = (const S *)p.pop;
-    const size_t N = p.N;
+    const uint64_t NP = p.NP;
 #pragma unroll
     for (int i = 0; i < 19; i++) {
-        if (Q == 0 || i == 0) f[i] = Pop<S>::ld(pop + (size_t)OPP(i) * N + n);
-        else f[i] = Pop<S>::ld(pop + (size_t)i * N + (uint32_t)((int32_t)n + nb.off(CX(i), CY(i), CZ(i))));
+        if (Q == 0 || i == 0) f[i] = Pop<S>::ld(pop + (uint64_t)OPP(i) * NP + n);
+        else f[i] = Pop<S>::ld(pop + (uint64_t)i * NP + (uint32_t)((int32_t)n + nb.off(CX(i), CY(i), CZ(i))));
     }
 }
 
@@ -240,14 +301,13 @@ __device__ __forceinline__ void load_prev_out(const LatParams &p, uint32_t n, co
 // skipping targets that leave a non-periodic domain (shader.rs:273-305)
 template <class S, int Q>
 __device__ __forceinline__ void store_prev_out(const LatParams &p, uint32_t n, uint32_t x, uint32_t y, uint32_t z, const Nb &nb,
-                                               const typename Pop<S>::real *f, uint32_t seed) {
+                                               const typename Pop<S>::real *f, Rng &rng) {
     S *pop = (S *)p.pop;
-    const size_t N = p.N;
-    const uint32_t key0 = n * 19u;
+    const uint64_t NP = p.NP;
 #pragma unroll
     for (int i = 0; i < 19; i++) {
         if (Q == 0 || i == 0) {
-            Pop<S>::st(pop + (size_t)OPP(i) * N + n, f[i], key0 + (uint32_t)OPP(i), seed);
+            pop[(uint64_t)OPP(i) * NP + n] = Pop<S>::enc(f[i], rng);
         } else {
             bool ok = true;
             if (CX(i) == 1) ok = ok && (p.per[0] || x < p.NX - 1);
@@ -256,7 +316,8 @@ __device__ __forceinline__ void store_prev_out(const LatParams &p, uint32_t n, u
             if (CY(i) == -1) ok = ok && (p.per[1] || y > 0);
             if (CZ(i) == 1) ok = ok && (p.per[2] || z < p.NZ - 1);
             if (CZ(i) == -1) ok = ok && (p.per[2] || z > 0);
-            if (ok) Pop<S>::st(pop + (size_t)i * N + (uint32_t)((int32_t)n + nb.off(CX(i), CY(i), CZ(i))), f[i], key0 + (uint32_t)i, seed);
+            const auto v = Pop<S>::enc(f[i], rng);
+            if (ok) pop[(uint64_t)i * NP + (uint32_t)((int32_t)n + nb.off(CX(i), CY(i), CZ(i)))] = v;
         }
     }
 }
@@ -296,48 +357,57 @@ struct Moments {
     R rho1, jx, jy, jz, sxx, syy, szz, sxy, sxz, syz;
 };
 
+// shader.rs:341-365, from the sums s_k and differences d_k of the 9
+// opposite pairs (2k+1, 2k+2)
 template <class R>
 __device__ __forceinline__ Moments<R> moments(const R *f) {
-    Moments<R> m{};
+    R s[9], d[9];
 #pragma unroll
-    for (int i = 0; i < 19; i++) {
-        m.rho1 += f[i];
-        if (CX(i)) m.jx += (R)CX(i) * f[i];
-        if (CY(i)) m.jy += (R)CY(i) * f[i];
-        if (CZ(i)) m.jz += (R)CZ(i) * f[i];
-        if (CX(i)) m.sxx += f[i];
-        if (CY(i)) m.syy += f[i];
-        if (CZ(i)) m.szz += f[i];
-        if (CX(i) * CY(i)) m.sxy += (R)(CX(i) * CY(i)) * f[i];
-        if (CX(i) * CZ(i)) m.sxz += (R)(CX(i) * CZ(i)) * f[i];
-        if (CY(i) * CZ(i)) m.syz += (R)(CY(i) * CZ(i)) * f[i];
-    }
+    for (int k = 0; k < 9; k++) { s[k] = f[2 * k + 1] + f[2 * k + 2]; d[k] = f[2 * k + 1] - f[2 * k + 2]; }
+    Moments<R> m;
+    m.rho1 = f[0] + ((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7])) + s[8];
+    // odd members: 1 (1,0,0) 3 (0,1,0) 5 (0,0,1) 7 (1,1,0) 9 (1,0,1) 11 (0,1,1) 13 (1,-1,0) 15 (1,0,-1) 17 (0,1,-1)
+    m.jx = (d[0] + d[3]) + (d[4] + d[6]) + d[7];
+    m.jy = (d[1] + d[3]) + (d[5] - d[6]) + d[8];
+    m.jz = (d[2] + d[4]) + (d[5] - d[7]) - d[8];
+    m.sxx = (s[0] + s[3]) + (s[4] + s[6]) + s[7];
+    m.syy = (s[1] + s[3]) + (s[5] + s[6]) + s[8];
+    m.szz = (s[2] + s[4]) + (s[5] + s[7]) + s[8];
+    m.sxy = s[3] - s[6];
+    m.sxz = s[4] - s[7];
+    m.syz = s[5] - s[8];
     return m;
 }
 
 // shader.rs:818-824: non-equilibrium stress from shifted moments
 template <class R>
 __device__ __forceinline__ void pi_neq(const Moments<R> &m, R rho, R ux, R uy, R uz, R *pi) {
-    pi[0] = m.sxx - rho * ux * ux - m.rho1 / (R)3;
-    pi[1] = m.syy - rho * uy * uy - m.rho1 / (R)3;
-    pi[2] = m.szz - rho * uz * uz - m.rho1 / (R)3;
+    const R r3 = m.rho1 / (R)3;
+    pi[0] = m.sxx - rho * ux * ux - r3;
+    pi[1] = m.syy - rho * uy * uy - r3;
+    pi[2] = m.szz - rho * uz * uz - r3;
     pi[3] = m.sxy - rho * ux * uy;
     pi[4] = m.sxz - rho * ux * uz;
     pi[5] = m.syz - rho * uy * uz;
 }
 
-// shader.rs:528-538
+// shader.rs:528-538: 0 outside the sponge layers, rising linearly to 1 at a
+// face; the layer test is done on integers first, and the ramps multiply by
+// reciprocal widths
 template <class R>
 __device__ __forceinline__ R sponge_at(const Consts<R> &k, const LatParams &p, uint32_t x, uint32_t y, uint32_t z) {
-    R pos[3] = {(R)x, (R)y, (R)z};
-    R hi[3] = {(R)(p.NX - 1) - pos[0], (R)(p.NY - 1) - pos[1], (R)(p.NZ - 1) - pos[2]};
+    const bool in = x < p.sp_w[0] || p.NX - 1 - x < p.sp_w[1] || y < p.sp_w[2] || p.NY - 1 - y < p.sp_w[3] || z < p.sp_w[4] ||
+                    p.NZ - 1 - z < p.sp_w[5];
+    if (!in) return (R)0;
+    const R pos[3] = {(R)x, (R)y, (R)z};
+    const R hi[3] = {(R)(p.NX - 1 - x), (R)(p.NY - 1 - y), (R)(p.NZ - 1 - z)};
     R s = 0;
 #pragma unroll
     for (int a = 0; a < 3; a++) {
-        if (k.sp_lo[a] > (R)0) s = max(s, (R)1 - pos[a] / k.sp_lo[a]);
-        if (k.sp_hi[a] > (R)0) s = max(s, (R)1 - hi[a] / k.sp_hi[a]);
+        if (k.sp_lo[a] > (R)0) s = max(s, (R)1 - pos[a] * k.sp_lo_inv[a]);
+        if (k.sp_hi[a] > (R)0) s = max(s, (R)1 - hi[a] * k.sp_hi_inv[a]);
     }
-    return min(max(s, (R)0), (R)1);
+    return min(s, (R)1);
 }
 
 }  // namespace lbm
