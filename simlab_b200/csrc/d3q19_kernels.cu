@@ -103,10 +103,18 @@ __device__ R wall_tau(const LatParams &p, const Consts<R> &k, uint32_t r, uint32
 // are each split into a part even in c (the same for i and o) and a part odd
 // in c (opposite signs); with per-weight-class coefficients a pair costs a
 // handful of instructions.
-template <class R, int COLL, int SC = 1>
+//
+// FEAT selects compile-time feature sets for the hot loop: 0 reads every
+// switch from the parameters; odd values fix forcing and the u_inf absorbing
+// target off and LES to bit 1.
+template <class R, int COLL, int SC = 1, int FEAT = 0>
 __device__ __forceinline__ void relax(const LatParams &p, const Consts<R> &k, R *f, uint32_t x, uint32_t y, uint32_t z,
                                       bool wall, uint32_t r, uint32_t mask, R pcx, R pcy, R pcz, const R *om, R &rho_o, R &ux_o,
                                       R &uy_o, R &uz_o) {
+    constexpr bool SPEC = (FEAT & 1) != 0;
+    const bool les_on = SPEC ? (FEAT & 2) != 0 : (p.les_on != 0);
+    const bool forcing = SPEC ? false : (p.forcing != 0);
+    const bool abs_u = SPEC ? false : (p.abs_u != 0);
     const R isc = (R)(1.0 / SC);
     Moments<R> m = moments<R>(f);
     if (SC != 1) {
@@ -121,7 +129,7 @@ __device__ __forceinline__ void relax(const LatParams &p, const Consts<R> &k, R 
     R pi[6];
     pi_neq<R>(m, rho, ux, uy, uz, pi);
     R tau = k.tau0;
-    if (p.les_on) {
+    if (les_on) {
         // Smagorinsky tau from |Pi_neq| (shader.rs:825-828)
         const R pp = pi[0] * pi[0] + pi[1] * pi[1] + pi[2] * pi[2] + (R)2 * (pi[3] * pi[3] + pi[4] * pi[4] + pi[5] * pi[5]);
         const R qn = sqrt((R)2 * pp);
@@ -139,7 +147,7 @@ __device__ __forceinline__ void relax(const LatParams &p, const Consts<R> &k, R 
     const R sg = k.sigma * sp * sp;  // absorbing strength (0 outside the layers)
     const R tr = (pi[0] + pi[1] + pi[2]) * (R)(1.0 / 3.0);
     R Gx = 0, Gy = 0, Gz = 0, uG = 0, fo = 0;
-    if (p.forcing) {
+    if (forcing) {
         Gx = rho * k.grav[0]; Gy = rho * k.grav[1]; Gz = rho * k.grav[2];
         uG = ux * Gx + uy * Gy + uz * Gz;
         fo = (R)1 - (R)0.5 * omg;
@@ -156,7 +164,7 @@ __device__ __forceinline__ void relax(const LatParams &p, const Consts<R> &k, R 
     const R Bq = m.rho1 - rho * usq;
     const R lam = COLL == 1 ? omg : (R)1;
     R cA, cB, cO, dB;  // coefficient multipliers (unit weight) and the constant shift
-    if (p.abs_u) {
+    if (abs_u) {
         const R l2 = lam - sg;
         cA = l2 * (R)4.5 * rho;
         cB = l2 * Bq;
@@ -180,8 +188,8 @@ __device__ __forceinline__ void relax(const LatParams &p, const Consts<R> &k, R 
         R v = w0 * (cB + dB);
         if (COLL == 1) v = v + om1 * f[0];
         else v = v - ((R)4.5 * w0 * om1) * tr;
-        if (p.abs_u) v = v + sgsc * k.ft_rest;
-        if (p.forcing) v = v + w0 * (fo * ((R)-3 * uG));
+        if (abs_u) v = v + sgsc * k.ft_rest;
+        if (forcing) v = v + w0 * (fo * ((R)-3 * uG));
         f[0] = v;
     }
 #pragma unroll
@@ -191,7 +199,7 @@ __device__ __forceinline__ void relax(const LatParams &p, const Consts<R> &k, R 
         const R cu = cdot<R>(i, ux, uy, uz);
         R even = (axis ? A_a : A_e) * (cu * cu) + (axis ? B_a : B_e);
         R odd = (axis ? O_a : O_e) * cu;
-        if (p.abs_u) {
+        if (abs_u) {
             even = even + sgsc * k.ft_even[kk];
             odd = odd + sgsc * k.ft_odd[kk];
         }
@@ -216,7 +224,7 @@ __device__ __forceinline__ void relax(const LatParams &p, const Consts<R> &k, R 
             vi = en + odd;
             vo = en - odd;
         }
-        if (p.forcing) {
+        if (forcing) {
             const R w = axis ? wa : we;
             const R cg = cdot<R>(i, Gx, Gy, Gz);
             const R fe_ = w * (fo * ((R)9 * cu * cg - (R)3 * uG));
@@ -248,7 +256,7 @@ __global__ void __launch_bounds__(BLOCK) k_bulk(const __grid_constant__ LatParam
     R rho, ux, uy, uz;
     const R om0[3] = {0, 0, 0};
     relax<R, COLL>(p, k, f, x, y, z, false, 0, 0, 0, 0, 0, om0, rho, ux, uy, uz);
-    Rng rng{sr_hash(n, s.seed)};
+    Rng rng{sr_hash_mix(n, s.seed_mix)};
     store_out<S, P>(p, n, nb, f, rng);
 }
 
@@ -373,7 +381,7 @@ __device__ __noinline__ void zwrap_cell(const LatParams &p, const StepParams &s,
     R rho, ux, uy, uz;
     const R om0[3] = {0, 0, 0};
     relax<R, COLL>(p, K<R>(p), f, x, y, z, false, 0, 0, 0, 0, 0, om0, rho, ux, uy, uz);
-    Rng rng{sr_hash(n, s.seed)};
+    Rng rng{sr_hash_mix(n, s.seed_mix)};
 #pragma unroll
     for (int i = 0; i < 19; i++) {
         const S v = Pop<S>::enc(f[i], rng);
@@ -382,7 +390,7 @@ __device__ __noinline__ void zwrap_cell(const LatParams &p, const StepParams &s,
     }
 }
 
-template <class S, int P, int COLL>
+template <class S, int P, int COLL, int FEAT>
 __global__ void __launch_bounds__(BLOCK, sizeof(S) == 8 ? 2 : 3) k_bulk_tma(const __grid_constant__ LatParams p, const __grid_constant__ StepParams s) {
     using R = typename Pop<S>::real;
     constexpr uint32_t T = Tile<S>::cells, SLOT = slot_bytes<S>(), BUF = buf_bytes<S>();
@@ -502,8 +510,8 @@ __global__ void __launch_bounds__(BLOCK, sizeof(S) == 8 ? 2 : 3) k_bulk_tma(cons
             }
             R rho, ux, uy, uz;
             const R om0[3] = {0, 0, 0};
-            relax<R, COLL, SC>(p, k, f, x, y, z, false, 0, 0, 0, 0, 0, om0, rho, ux, uy, uz);
-            Rng rng{sr_hash(n, s.seed)};
+            relax<R, COLL, SC, FEAT>(p, k, f, x, y, z, false, 0, 0, 0, 0, 0, om0, rho, ux, uy, uz);
+            Rng rng{sr_hash_mix(n, s.seed_mix)};
             S out[19];
             if constexpr (SC != 1) {
                 // stochastic rounding noise per value, then one packed
@@ -603,7 +611,7 @@ __global__ void __launch_bounds__(BLOCK) k_walls(const __grid_constant__ LatPara
                 for (int a = 0; a < 3; a++) { Fo[a] += Rec<R>::ft(p, r, a); To[a] += Rec<R>::ft(p, r, 3 + a); }
             }
             for (int a = 0; a < 3; a++) { Rec<R>::set_ft(p, r, a, Fo[a]); Rec<R>::set_ft(p, r, 3 + a, To[a]); }
-            Rng rng{sr_hash(cell, s.seed)};
+            Rng rng{sr_hash_mix(cell, s.seed_mix)};
             store_out<S, P>(p, cell, nb, f, rng);
         } else {
             for (int a = 0; a < 3; a++) { Fo[a] = Rec<R>::ft(p, r, a); To[a] = Rec<R>::ft(p, r, 3 + a); }
@@ -689,7 +697,7 @@ __global__ void __launch_bounds__(BLOCK) k_faces(const __grid_constant__ LatPara
         if ((fg & 3u) == 0u) {
             R g[19];
             load_prev_out<S, Q>(p, m, nbm, g);
-            switch (info >> 2) {
+            switch ((info >> 2) & 7u) {
                 case 1: mirror<R, 1>(g, f); break;
                 case 2: mirror<R, 2>(g, f); break;
                 case 3: mirror<R, 3>(g, f); break;
@@ -734,8 +742,8 @@ __global__ void __launch_bounds__(BLOCK) k_faces(const __grid_constant__ LatPara
         for (int i = 0; i < 19; i++) f[i] = feq_i<R>(i, rho1, rho, ux, uy, uz, usq) + fneq_i<R>(i, pi, tr);
     }
     const Nb nbb = make_nb(p, x, y, z);
-    Rng rng{sr_hash(b, s.seed)};
-    store_prev_out<S, Q>(p, b, x, y, z, nbb, f, rng);
+    Rng rng{sr_hash_mix(b, s.seed_mix)};
+    store_prev_out<S, Q>(p, b, nbb, info >> 8, f, rng);
 }
 
 // ---------------------------------------------------------------- init
@@ -916,11 +924,11 @@ static int num_sms() {
 }
 
 // persistent grid of the staged kernel: resident blocks per SM x SMs
-template <class S, int P, int COLL>
+template <class S, int P, int COLL, int FEAT>
 static unsigned tma_grid() {
     static unsigned g = 0;
     if (!g) {
-        auto kern = k_bulk_tma<S, P, COLL>;
+        auto kern = k_bulk_tma<S, P, COLL, FEAT>;
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem<S>());
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BLOCK, tma_smem<S>());
@@ -929,16 +937,37 @@ static unsigned tma_grid() {
     return g;
 }
 
+template <class S, int P, int COLL, int FEAT>
+static void launch_tma(const LatParams &p, const StepParams &s, cudaStream_t st) {
+    const unsigned ntiles = (unsigned)((p.N + Tile<S>::cells - 1) / Tile<S>::cells);
+    k_bulk_tma<S, P, COLL, FEAT><<<std::min(ntiles, tma_grid<S, P, COLL, FEAT>()), BLOCK, tma_smem<S>(), st>>>(p, s);
+}
+
+// one step: faces, wall cells (on the side stream `side` when they cannot
+// touch the faces' slots, overlapping the face kernel), then the bulk
 template <class S, int P, int COLL>
-static cudaError_t step_t(const LatParams &p, const StepParams &s, cudaStream_t st, cudaEvent_t *ev) {
+static cudaError_t step_t(const LatParams &p, const StepParams &s, cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join,
+                          cudaEvent_t *ev) {
     if (ev) cudaEventRecord(ev[0], st);
+    const bool overlap = side && p.nrec && p.nface;
+    if (overlap) {
+        cudaEventRecord(fork, st);
+        cudaStreamWaitEvent(side, fork, 0);
+        k_walls<S, P, COLL><<<blocks_for(p.nrec), BLOCK, 0, side>>>(p, s);
+        cudaEventRecord(join, side);
+    }
     if (p.nface) k_faces<S, P><<<blocks_for(p.nface), BLOCK, 0, st>>>(p, s);
     if (ev) cudaEventRecord(ev[1], st);
-    if (p.nrec) k_walls<S, P, COLL><<<blocks_for(p.nrec), BLOCK, 0, st>>>(p, s);
+    if (overlap) cudaStreamWaitEvent(st, join, 0);
+    else if (p.nrec) k_walls<S, P, COLL><<<blocks_for(p.nrec), BLOCK, 0, st>>>(p, s);
     if (ev) cudaEventRecord(ev[2], st);
     if (p.tma) {
-        const unsigned ntiles = (unsigned)((p.N + Tile<S>::cells - 1) / Tile<S>::cells);
-        k_bulk_tma<S, P, COLL><<<std::min(ntiles, tma_grid<S, P, COLL>()), BLOCK, tma_smem<S>(), st>>>(p, s);
+        if (!p.forcing && !p.abs_u) {
+            if (p.les_on) launch_tma<S, P, COLL, 3>(p, s, st);
+            else launch_tma<S, P, COLL, 1>(p, s, st);
+        } else {
+            launch_tma<S, P, COLL, 0>(p, s, st);
+        }
     } else {
         k_bulk<S, P, COLL><<<blocks_for(p.N), BLOCK, 0, st>>>(p, s);
     }
@@ -947,17 +976,19 @@ static cudaError_t step_t(const LatParams &p, const StepParams &s, cudaStream_t 
 }
 
 template <class S>
-static cudaError_t step_s(const LatParams &p, const StepParams &s, int parity, int coll, cudaStream_t st, cudaEvent_t *ev) {
-    if (parity == 0) return coll == 1 ? step_t<S, 0, 1>(p, s, st, ev) : step_t<S, 0, 0>(p, s, st, ev);
-    return coll == 1 ? step_t<S, 1, 1>(p, s, st, ev) : step_t<S, 1, 0>(p, s, st, ev);
+static cudaError_t step_s(const LatParams &p, const StepParams &s, int parity, int coll, cudaStream_t st, cudaStream_t side, cudaEvent_t fork,
+                          cudaEvent_t join, cudaEvent_t *ev) {
+    if (parity == 0) return coll == 1 ? step_t<S, 0, 1>(p, s, st, side, fork, join, ev) : step_t<S, 0, 0>(p, s, st, side, fork, join, ev);
+    return coll == 1 ? step_t<S, 1, 1>(p, s, st, side, fork, join, ev) : step_t<S, 1, 0>(p, s, st, side, fork, join, ev);
 }
 
-cudaError_t launch_step(int storage, const LatParams &p, const StepParams &s, int parity, int coll, cudaStream_t st, cudaEvent_t *ev) {
+cudaError_t launch_step(int storage, const LatParams &p, const StepParams &s, int parity, int coll, cudaStream_t st, cudaStream_t side,
+                        cudaEvent_t fork, cudaEvent_t join, cudaEvent_t *ev) {
     switch (storage) {
-        case 0: return step_s<float>(p, s, parity, coll, st, ev);
-        case 1: return step_s<__half>(p, s, parity, coll, st, ev);
-        case 2: return step_s<__nv_bfloat16>(p, s, parity, coll, st, ev);
-        case 3: return step_s<double>(p, s, parity, coll, st, ev);
+        case 0: return step_s<float>(p, s, parity, coll, st, side, fork, join, ev);
+        case 1: return step_s<__half>(p, s, parity, coll, st, side, fork, join, ev);
+        case 2: return step_s<__nv_bfloat16>(p, s, parity, coll, st, side, fork, join, ev);
+        case 3: return step_s<double>(p, s, parity, coll, st, side, fork, join, ev);
     }
     return cudaErrorInvalidValue;
 }

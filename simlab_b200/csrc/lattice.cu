@@ -64,6 +64,8 @@ struct lbm_lattice {
     lbm_setup setup{};
     lbm::LatParams lp{};
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;  // wall-cell kernel, when it cannot touch the faces' slots
+    cudaEvent_t fork = nullptr, join = nullptr;
     int device = 0;
     std::vector<void *> allocs;
     uint64_t steps_done = 0;
@@ -101,6 +103,10 @@ struct lbm_lattice {
         if (err_host) cudaFreeHost(err_host);
         if (ev) cudaEventDestroy(ev);
         for (cudaEvent_t e : prof_ev) cudaEventDestroy(e);
+        if (side) cudaStreamSynchronize(side);
+        if (fork) cudaEventDestroy(fork);
+        if (join) cudaEventDestroy(join);
+        if (side) cudaStreamDestroy(side);
         if (stream) cudaStreamDestroy(stream);
     }
     void wait() {
@@ -176,6 +182,7 @@ void fill_consts(lbm::Consts<R> &k, const lbm_setup &st) {
 lbm::StepParams step_params(const lbm_lattice *h, const lbm_step_in &s, uint32_t slot, uint64_t step_index) {
     lbm::StepParams sp{};
     sp.seed = (uint32_t)step_index * 2654435761u;  // lattice.rs:676
+    sp.seed_mix = sp.seed * 0x85EBCA77u + 0x632BE5ABu;
     sp.slot = slot;
     for (int a = 0; a < 3; a++) {
         sp.omega[a] = (float)s.omega[a];
@@ -214,32 +221,70 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     // otherwise the later face in -x,+x,-y,+y,-z,+z order wins; free-slip
     // faces collect their mirror axes.
     std::vector<uint32_t> faces;
-    std::vector<uint8_t> finfo;
-    auto face_type = [&](uint64_t x, uint64_t y, uint64_t z, uint8_t &info) -> bool {
+    std::vector<uint32_t> finfo;
+    auto face_type = [&](uint64_t x, uint64_t y, uint64_t z, uint32_t &info) -> bool {
         bool on[6] = {x == 0, x == NX - 1, y == 0, y == NY - 1, z == 0, z == NZ - 1};
         int ty = -1;
-        uint8_t mir = 0;
+        uint32_t mir = 0;
         for (int f = 0; f < 6; f++) {
             if (on[f] && st.faces[f] != LBM_FACE_PERIODIC) {
                 int t = st.faces[f] == LBM_FACE_VELOCITY ? 0 : (st.faces[f] == LBM_FACE_OPEN ? 1 : 2);
-                if (st.faces[f] == LBM_FACE_FREE_SLIP) mir |= (uint8_t)(1u << (f / 2));
+                if (st.faces[f] == LBM_FACE_FREE_SLIP) mir |= 1u << (f / 2);
                 ty = (ty == 0) ? 0 : t;
             }
         }
         if (ty < 0) return false;
-        info = (uint8_t)(ty | (ty == 2 ? (mir << 2) : 0));
+        info = (uint32_t)ty | (ty == 2 ? (mir << 2) : 0u);
         return true;
+    };
+    // a face cell's populations matter only where they stream into a cell
+    // that collides: bit i of the store mask is set when x + c_i is inside
+    // the domain (periodic axes wrap) and not itself a face cell
+    const uint64_t dimv[3] = {NX, NY, NZ};
+    auto on_face = [&](const int64_t c[3]) {
+        for (int a = 0; a < 3; a++)
+            if (!per[a] && (c[a] == 0 || c[a] == (int64_t)dimv[a] - 1)) return true;
+        return false;
+    };
+    auto store_mask = [&](uint64_t x, uint64_t y, uint64_t z) {
+        uint32_t mask = 0;
+        for (int i = 0; i < 19; i++) {
+            int64_t c[3] = {(int64_t)x + lbm::CX(i), (int64_t)y + lbm::CY(i), (int64_t)z + lbm::CZ(i)};
+            bool ok = true;
+            for (int a = 0; a < 3; a++) {
+                if (c[a] < 0 || c[a] >= (int64_t)dimv[a]) {
+                    if (!per[a]) ok = false;
+                    else c[a] = (c[a] + (int64_t)dimv[a]) % (int64_t)dimv[a];
+                }
+            }
+            if (ok && !on_face(c)) mask |= 1u << i;
+        }
+        return mask;
     };
     for (uint64_t z = 0; z < NZ; z++)
         for (uint64_t y = 0; y < NY; y++) {
             bool edge = y == 0 || y == NY - 1 || z == 0 || z == NZ - 1;
             auto visit = [&](uint64_t x) {
-                uint8_t info;
-                if (face_type(x, y, z, info)) { faces.push_back((uint32_t)((z * NY + y) * NX + x)); finfo.push_back(info); }
+                uint32_t info;
+                if (face_type(x, y, z, info)) {
+                    faces.push_back((uint32_t)((z * NY + y) * NX + x));
+                    finfo.push_back(info | (store_mask(x, y, z) << 8));
+                }
             };
             if (edge) { for (uint64_t x = 0; x < NX; x++) visit(x); }
             else { visit(0); visit(NX - 1); }
         }
+    // face cells are independent; grouping them by kind and store mask keeps
+    // each warp on one code path
+    {
+        std::vector<size_t> ord(faces.size());
+        for (size_t k = 0; k < ord.size(); k++) ord[k] = k;
+        std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return finfo[a] < finfo[b]; });
+        std::vector<uint32_t> f2(faces.size()), i2(faces.size());
+        for (size_t k = 0; k < ord.size(); k++) { f2[k] = faces[ord[k]]; i2[k] = finfo[ord[k]]; }
+        faces.swap(f2);
+        finfo.swap(i2);
+    }
     h->nface = (uint32_t)faces.size();
 
     // wall records (lattice.rs:454-482; record_words 202-218)
@@ -337,7 +382,7 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     p.recs = (uint32_t *)h->dalloc(nrec * lbm::RS * 4);
     p.recd = st.storage == LBM_STORAGE_FP64 ? (double *)h->dalloc(nrec * lbm::RD * 8) : nullptr;
     p.faces = (uint32_t *)h->dalloc(faces.size() * 4);
-    p.face_info = (uint8_t *)h->dalloc(finfo.size());
+    p.face_info = (uint32_t *)h->dalloc(finfo.size() * 4);
     const uint64_t nwb = (nrec + lbm::BLOCK - 1) / lbm::BLOCK;
     p.partials = (double *)h->dalloc(std::max<uint64_t>(nwb, 1) * 8 * sizeof(double));
     p.ticket = (uint32_t *)h->dalloc(16);
@@ -369,6 +414,36 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     p.moving = 0;
     fill_consts<float>(p.kf, st);
     fill_consts<double>(p.kd, st);
+    // sponge ramps per axis (shader.rs:528-538): 1 - p / width inside a layer
+    std::vector<float> tabf;
+    std::vector<double> tabd;
+    for (int a = 0; a < 3; a++) {
+        const uint64_t na = st.dims[a];
+        for (uint64_t q = 0; q < na; q++) {
+            float sf = 0.f;
+            double sd = 0.0;
+            const float pf = (float)q, hf = (float)(na - 1) - pf;
+            if (st.sponge[2 * a] > 0) { sf = std::max(sf, 1.0f - pf / (float)st.sponge[2 * a]); sd = std::max(sd, 1.0 - (double)q / st.sponge[2 * a]); }
+            if (st.sponge[2 * a + 1] > 0) {
+                sf = std::max(sf, 1.0f - hf / (float)st.sponge[2 * a + 1]);
+                sd = std::max(sd, 1.0 - (double)(na - 1 - q) / st.sponge[2 * a + 1]);
+            }
+            tabf.push_back(std::min(sf, 1.0f));
+            tabd.push_back(std::min(sd, 1.0));
+        }
+    }
+    p.sp_tab = (const float *)h->dalloc(tabf.size() * 4);
+    p.sp_tabd = (const double *)h->dalloc(tabd.size() * 8);
+    // the wall kernel may overlap the face kernel when no wall cell is within
+    // three cells of a non-periodic boundary (its slots then never meet the
+    // faces' slots or the inner cells the faces read)
+    bool walls_far = nrec > 0 && !faces.empty();
+    for (uint64_t r = 0; walls_far && r < nrec; r++) {
+        const uint64_t c = geom->walls[r].cell;
+        const uint64_t q[3] = {c % NX, (c / NX) % NY, c / (NX * NY)};
+        for (int a = 0; a < 3; a++)
+            if (!per[a] && (q[a] < 3 || q[a] + 4 > st.dims[a])) walls_far = false;
+    }
 
     cudaStream_t s = h->stream;
     ck(cudaMemsetAsync(p.pop, 0, h->pop_bytes, s), "memset");
@@ -379,10 +454,17 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     if (!wordsd.empty()) ck(cudaMemcpyAsync(p.recd, wordsd.data(), wordsd.size() * 8, cudaMemcpyHostToDevice, s), "upload records");
     if (!faces.empty()) {
         ck(cudaMemcpyAsync((void *)p.faces, faces.data(), faces.size() * 4, cudaMemcpyHostToDevice, s), "upload faces");
-        ck(cudaMemcpyAsync((void *)p.face_info, finfo.data(), finfo.size(), cudaMemcpyHostToDevice, s), "upload faces");
+        ck(cudaMemcpyAsync((void *)p.face_info, finfo.data(), finfo.size() * 4, cudaMemcpyHostToDevice, s), "upload faces");
     }
     if (!vbuf.empty()) ck(cudaMemcpyAsync(h->verts, vbuf.data(), vbuf.size() * 4, cudaMemcpyHostToDevice, s), "upload vertices");
     ck(cudaMemcpyAsync(h->slicedef, sd.data(), sd.size() * 4, cudaMemcpyHostToDevice, s), "upload slices");
+    ck(cudaMemcpyAsync((void *)p.sp_tab, tabf.data(), tabf.size() * 4, cudaMemcpyHostToDevice, s), "upload sponge");
+    ck(cudaMemcpyAsync((void *)p.sp_tabd, tabd.data(), tabd.size() * 8, cudaMemcpyHostToDevice, s), "upload sponge");
+    if (walls_far) {
+        ck(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking), "cudaStreamCreate");
+        ck(cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming), "cudaEventCreate");
+        ck(cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming), "cudaEventCreate");
+    }
     ck(cudaMemsetAsync(p.ticket, 0, 16, s), "memset");
     ck(cudaMemsetAsync(p.hist, 0, KMAX * 8 * sizeof(double), s), "memset");
     ck(cudaMemsetAsync(h->vacc, 0, std::max<uint64_t>(h->nvert, 1) * 2 * sizeof(double), s), "memset");
@@ -414,7 +496,8 @@ void run_impl(lbm_lattice *h, const lbm_step_in *steps, uint64_t n, double *forc
                 evs = h->prof_ev.data() + 4 * h->prof_steps;
                 h->prof_steps++;
             }
-            ck(lbm::launch_step(h->setup.storage, p, sp, (int)(idx % 2), h->setup.collision, h->stream, evs), "step kernels");
+            ck(lbm::launch_step(h->setup.storage, p, sp, (int)(idx % 2), h->setup.collision, h->stream, h->side, h->fork, h->join, evs),
+               "step kernels");
             if (si.sample && (h->nvert || h->npix))
                 ck(lbm::launch_sample(h->setup.storage, p, sp, (int)(idx % 2), h->verts, h->nvert, h->voff, h->vacc, h->slicedef,
                                       h->nslices, h->npix, h->sacc, h->stream),

@@ -94,7 +94,7 @@ struct LatParams {
     uint32_t *recs;            // nrec * RS words
     double *recd;              // FP64 engine: nrec * RD doubles (else null)
     const uint32_t *faces;     // face cells
-    const uint8_t *face_info;  // kind (0 velocity, 1 open, 2 free slip) | mirror axes << 2
+    const uint32_t *face_info; // kind (0 velocity, 1 open, 2 free slip) | mirror axes << 2 | store mask << 8
     double *partials;          // per wall block: 8 doubles
     uint32_t *ticket;          // last-block counter of the force reduction
     double *hist;              // per step slot: 8 doubles (F, T)
@@ -107,6 +107,8 @@ struct LatParams {
     int per[3];
     int abs_u, total_p, wall_model, forcing, sponge_on, les_on, moving;
     uint32_t sp_w[6];          // sponge widths in cells, -x,+x,-y,+y,-z,+z
+    const float *sp_tab;       // sponge ramp per x, then per y, then per z (NX + NY + NZ values)
+    const double *sp_tabd;     // the same in FP64
     int tma;                   // the staged bulk kernel applies (NX * element size % 16 == 0)
     Consts<float> kf;
     Consts<double> kd;
@@ -114,6 +116,7 @@ struct LatParams {
 
 struct StepParams {
     uint32_t seed;   // stochastic rounding seed of this step (lattice.rs:676)
+    uint32_t seed_mix;  // seed * 0x85EBCA77 + 0x632BE5AB, the seed's term of sr_hash
     uint32_t slot;   // history slot of this step
     float omega[3];  // angular velocity, rad per step
     double omega_d[3];
@@ -136,6 +139,11 @@ template <> __device__ __forceinline__ const Consts<double> &K<double>(const Lat
 // Recipes constants) whose top bits serve the cell's stores in turn.
 __host__ __device__ __forceinline__ uint32_t sr_hash(uint32_t key, uint32_t seed) {
     uint32_t h = (key * 0x9E3779B1u) ^ (seed * 0x85EBCA77u + 0x632BE5ABu);
+    h ^= h >> 16; h *= 0x7feb352du; h ^= h >> 15; h *= 0x846ca68bu; h ^= h >> 16;
+    return h;
+}
+__device__ __forceinline__ uint32_t sr_hash_mix(uint32_t key, uint32_t mix) {
+    uint32_t h = (key * 0x9E3779B1u) ^ mix;
     h ^= h >> 16; h *= 0x7feb352du; h ^= h >> 15; h *= 0x846ca68bu; h ^= h >> 16;
     return h;
 }
@@ -297,28 +305,22 @@ __device__ __forceinline__ void load_prev_out(const LatParams &p, uint32_t n, co
     }
 }
 
-// writes a face cell's "previous" post-collision populations for parity Q,
-// skipping targets that leave a non-periodic domain (shader.rs:273-305)
+// writes a face cell's "previous" post-collision populations for parity Q
+// (shader.rs:273-305).  Only the directions in `mask` are written: those
+// that stream into a cell that collides.  The rest (leaving a non-periodic
+// domain, or entering another face cell, which never collides) are read by
+// no one.
 template <class S, int Q>
-__device__ __forceinline__ void store_prev_out(const LatParams &p, uint32_t n, uint32_t x, uint32_t y, uint32_t z, const Nb &nb,
+__device__ __forceinline__ void store_prev_out(const LatParams &p, uint32_t n, const Nb &nb, uint32_t mask,
                                                const typename Pop<S>::real *f, Rng &rng) {
     S *pop = (S *)p.pop;
     const uint64_t NP = p.NP;
 #pragma unroll
     for (int i = 0; i < 19; i++) {
-        if (Q == 0 || i == 0) {
-            pop[(uint64_t)OPP(i) * NP + n] = Pop<S>::enc(f[i], rng);
-        } else {
-            bool ok = true;
-            if (CX(i) == 1) ok = ok && (p.per[0] || x < p.NX - 1);
-            if (CX(i) == -1) ok = ok && (p.per[0] || x > 0);
-            if (CY(i) == 1) ok = ok && (p.per[1] || y < p.NY - 1);
-            if (CY(i) == -1) ok = ok && (p.per[1] || y > 0);
-            if (CZ(i) == 1) ok = ok && (p.per[2] || z < p.NZ - 1);
-            if (CZ(i) == -1) ok = ok && (p.per[2] || z > 0);
-            const auto v = Pop<S>::enc(f[i], rng);
-            if (ok) pop[(uint64_t)i * NP + (uint32_t)((int32_t)n + nb.off(CX(i), CY(i), CZ(i)))] = v;
-        }
+        if (!(mask & (1u << i))) continue;
+        const auto v = Pop<S>::enc(f[i], rng);
+        if (Q == 0 || i == 0) pop[(uint64_t)OPP(i) * NP + n] = v;
+        else pop[(uint64_t)i * NP + (uint32_t)((int32_t)n + nb.off(CX(i), CY(i), CZ(i)))] = v;
     }
 }
 
@@ -391,23 +393,16 @@ __device__ __forceinline__ void pi_neq(const Moments<R> &m, R rho, R ux, R uy, R
     pi[5] = m.syz - rho * uy * uz;
 }
 
-// shader.rs:528-538: 0 outside the sponge layers, rising linearly to 1 at a
-// face; the layer test is done on integers first, and the ramps multiply by
-// reciprocal widths
+// shader.rs:528-538: the sponge factor is the largest of six ramps, each
+// depending on one coordinate, so it is the largest of three per-axis values
+// tabulated at setup with the reference's arithmetic (1 - p / width)
+template <class R> __device__ __forceinline__ const R *sp_table(const LatParams &p);
+template <> __device__ __forceinline__ const float *sp_table<float>(const LatParams &p) { return p.sp_tab; }
+template <> __device__ __forceinline__ const double *sp_table<double>(const LatParams &p) { return p.sp_tabd; }
 template <class R>
-__device__ __forceinline__ R sponge_at(const Consts<R> &k, const LatParams &p, uint32_t x, uint32_t y, uint32_t z) {
-    const bool in = x < p.sp_w[0] || p.NX - 1 - x < p.sp_w[1] || y < p.sp_w[2] || p.NY - 1 - y < p.sp_w[3] || z < p.sp_w[4] ||
-                    p.NZ - 1 - z < p.sp_w[5];
-    if (!in) return (R)0;
-    const R pos[3] = {(R)x, (R)y, (R)z};
-    const R hi[3] = {(R)(p.NX - 1 - x), (R)(p.NY - 1 - y), (R)(p.NZ - 1 - z)};
-    R s = 0;
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        if (k.sp_lo[a] > (R)0) s = max(s, (R)1 - pos[a] * k.sp_lo_inv[a]);
-        if (k.sp_hi[a] > (R)0) s = max(s, (R)1 - hi[a] * k.sp_hi_inv[a]);
-    }
-    return min(s, (R)1);
+__device__ __forceinline__ R sponge_at(const Consts<R> &, const LatParams &p, uint32_t x, uint32_t y, uint32_t z) {
+    const R *t = sp_table<R>(p);
+    return max(max(__ldg(t + x), __ldg(t + p.NX + y)), __ldg(t + p.NX + p.NY + z));
 }
 
 }  // namespace lbm

@@ -7,9 +7,11 @@
 namespace lbm {
 
 // storage: 0 FP32, 1 FP16, 2 BF16, 3 FP64 (lbm_storage); coll: 0 regularized, 1 BGK
-// ev: null, or 4 events recorded before faces, before walls, before bulk, after bulk
-cudaError_t launch_step(int storage, const LatParams &p, const StepParams &s, int parity, int coll, cudaStream_t st,
-                        cudaEvent_t *ev = nullptr);
+// side: null, or a second stream on which the wall-cell kernel overlaps the
+// face kernel (fork/join: two events); ev: null, or 4 events recorded before
+// the step, after faces, after walls, after bulk
+cudaError_t launch_step(int storage, const LatParams &p, const StepParams &s, int parity, int coll, cudaStream_t st, cudaStream_t side,
+                        cudaEvent_t fork, cudaEvent_t join, cudaEvent_t *ev = nullptr);
 cudaError_t launch_init(int storage, const LatParams &p, cudaStream_t st);
 cudaError_t launch_dump(int storage, const LatParams &p, int q, cudaStream_t st);
 cudaError_t launch_sample(int storage, const LatParams &p, const StepParams &s, int q, const float *verts, uint32_t nvert, float voff,
