@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(BLOCK) k_bulk(const __grid_constant__ LatParam
     using R = typename Pop<S>::real;
     const uint32_t n = blockIdx.x * BLOCK + threadIdx.x;
     if (n >= p.N) return;
-    if (p.flags[n] != 0u) return;
+    if ((p.flags[n] & ~FLAG_XFACE) != 0u) return;
     uint32_t x, y, z;
     coords(p, n, x, y, z);
     const Nb nb = make_nb(p, x, y, z);
@@ -258,6 +258,98 @@ __global__ void __launch_bounds__(BLOCK) k_bulk(const __grid_constant__ LatParam
     relax<R, COLL>(p, k, f, x, y, z, false, 0, 0, 0, 0, 0, om0, rho, ux, uy, uz);
     Rng rng{sr_hash_mix(n, s.seed_mix)};
     store_out<S, P>(p, n, nb, f, rng);
+}
+
+// ---------------------------------------------------------------- faces
+template <class R, int M, int I>
+__device__ __forceinline__ void mirror_one(const R *g, R *f) {
+    constexpr int j = DIR((M & 1) ? -CX(I) : CX(I), (M & 2) ? -CY(I) : CY(I), (M & 4) ? -CZ(I) : CZ(I));
+    f[I] = g[j];
+}
+template <class R, int M, int... Is>
+__device__ __forceinline__ void mirror_all(const R *g, R *f, std::integer_sequence<int, Is...>) {
+    (mirror_one<R, M, Is>(g, f), ...);
+}
+template <class R, int M>
+__device__ __forceinline__ void mirror(const R *g, R *f) {
+    mirror_all<R, M>(g, f, std::make_integer_sequence<int, 19>{});
+}
+
+// A face cell's "previous" post-collision populations from its inner
+// neighbour's post-collision populations g (shader.rs:630-687): velocity
+// inlet (u = u_inf, or the far field's total pressure with u from inside),
+// open face (rho = 1), both as feq + fneq(Pi) of the neighbour's state; free
+// slip (no reference counterpart) as the neighbour's mirror image.  fluid:
+// the inner neighbour collides (else rest at u_inf).
+template <class R>
+__device__ __forceinline__ void face_values(const LatParams &p, const Consts<R> &k, uint32_t info, bool fluid, const R *g, R *f) {
+    if ((info & 3u) == 2u) {
+        if (fluid) {
+            switch ((info >> 2) & 7u) {
+                case 1: mirror<R, 1>(g, f); break;
+                case 2: mirror<R, 2>(g, f); break;
+                case 3: mirror<R, 3>(g, f); break;
+                case 4: mirror<R, 4>(g, f); break;
+                case 5: mirror<R, 5>(g, f); break;
+                case 6: mirror<R, 6>(g, f); break;
+                case 7: mirror<R, 7>(g, f); break;
+                default: mirror<R, 0>(g, f); break;
+            }
+        } else {
+            const R usq = (R)1.5 * (k.u_inf[0] * k.u_inf[0] + k.u_inf[1] * k.u_inf[1] + k.u_inf[2] * k.u_inf[2]);
+#pragma unroll
+            for (int i = 0; i < 19; i++) f[i] = feq_i<R>(i, (R)0, (R)1, k.u_inf[0], k.u_inf[1], k.u_inf[2], usq);
+        }
+        return;
+    }
+    R rho = 1, ux = k.u_inf[0], uy = k.u_inf[1], uz = k.u_inf[2];
+    R pi[6] = {0, 0, 0, 0, 0, 0};
+    if (fluid) {
+        const Moments<R> mo = moments<R>(g);
+        rho = (R)1 + mo.rho1;
+        ux = mo.jx / rho - (R)0.5 * k.grav[0];
+        uy = mo.jy / rho - (R)0.5 * k.grav[1];
+        uz = mo.jz / rho - (R)0.5 * k.grav[2];
+        pi_neq<R>(mo, rho, ux, uy, uz, pi);
+    }
+    if ((info & 3u) == 0u) {
+        if (p.total_p) {
+            const R uinf2 = k.u_inf[0] * k.u_inf[0] + k.u_inf[1] * k.u_inf[1] + k.u_inf[2] * k.u_inf[2];
+            rho = ((R)(1.0 / 3.0) + (R)0.5 * uinf2) / ((R)(1.0 / 3.0) + (R)0.5 * (ux * ux + uy * uy + uz * uz));
+        } else {
+            ux = k.u_inf[0]; uy = k.u_inf[1]; uz = k.u_inf[2];
+        }
+    } else {
+        rho = 1;
+    }
+    const R rho1 = rho - (R)1;
+    const R usq = (R)1.5 * (ux * ux + uy * uy + uz * uz);
+    const R tr = (pi[0] + pi[1] + pi[2]) * (R)(1.0 / 3.0);
+#pragma unroll
+    for (int i = 0; i < 19; i++) f[i] = feq_i<R>(i, rho1, rho, ux, uy, uz, usq) + fneq_i<R>(i, pi, tr);
+}
+
+template <class S, int P>
+__global__ void __launch_bounds__(BLOCK) k_faces(const __grid_constant__ LatParams p, const __grid_constant__ StepParams s) {
+    using R = typename Pop<S>::real;
+    constexpr int Q = 1 - P;
+    const uint32_t kf = blockIdx.x * BLOCK + threadIdx.x;
+    if (kf >= s.nface) return;
+    const uint32_t b = p.faces[kf];
+    const uint32_t info = p.face_info[kf];
+    uint32_t x, y, z;
+    coords(p, b, x, y, z);
+    uint32_t cx = x, cy = y, cz = z;
+    if (!p.per[0]) cx = min(max(cx, 1u), p.NX - 2);
+    if (!p.per[1]) cy = min(max(cy, 1u), p.NY - 2);
+    if (!p.per[2]) cz = min(max(cz, 1u), p.NZ - 2);
+    const uint32_t m = (cz * p.NY + cy) * p.NX + cx;
+    const bool fluid = (p.flags[m] & 3u) == 0u;
+    R g[19], f[19];
+    if (fluid) load_prev_out<S, Q>(p, m, make_nb(p, cx, cy, cz), g);
+    face_values<R>(p, K<R>(p), info, fluid, g, f);
+    Rng rng{sr_hash_mix(b, s.seed_mix)};
+    store_prev_out<S, Q>(p, b, make_nb(p, x, y, z), info >> 8, f, rng);
 }
 
 // ---------------------------------------------------------------- staged bulk
@@ -294,7 +386,8 @@ constexpr int CWARPS = 7, CTHREADS = CWARPS * 32;
 template <class S> struct Tile { static constexpr uint32_t cells = sizeof(S) == 2 ? 2 * CTHREADS : CTHREADS; };
 template <class S> constexpr uint32_t slot_bytes() { return Tile<S>::cells * (uint32_t)sizeof(S) + 16; }
 template <class S> constexpr uint32_t buf_bytes() { return 19 * slot_bytes<S>() + Tile<S>::cells * 4; }
-template <class S> constexpr uint32_t tma_smem() { return 2 * buf_bytes<S>() + 128; }  // + alignment slack
+constexpr int NBUF = 3;  // tile buffers per block: loads run up to two tiles ahead
+template <class S> constexpr uint32_t tma_smem() { return NBUF * buf_bytes<S>() + 128; }  // + alignment slack
 
 // element offset of plane j's first tile cell in its shared-memory slot
 template <class S, int P>
@@ -360,11 +453,95 @@ __device__ __forceinline__ void tma_load_tile(const LatParams &p, uint8_t *buf, 
     bulk_g2s(buf + 19 * SLOT, p.flags + n0, T * 4, bar);
 }
 
+// The x-face cell b next to cell m (b = m - 1 when x = 1, b = m + 1 when
+// x = NX - 2), on a planar x face whose inner neighbour is m: its populations
+// for the next step are what the face kernel of the next step would write
+// from m's post-collision state, so the thread that just collided m computes
+// them from its rounded outputs and writes them into b's slots of the staged
+// tile; they reach HBM with the tile.  Only the 5 directions entering the
+// domain are needed (the face kernel's store mask for a planar x face).
+__host__ __device__ __forceinline__ constexpr int inward_dir(bool lo, int q) {
+    // c_x = +1 directions (face at x = 0) or c_x = -1 (face at x = NX - 1), ascending
+    return lo ? (q == 0 ? 1 : (q == 1 ? 7 : (q == 2 ? 9 : (q == 3 ? 13 : 15)))) : (q == 0 ? 2 : (q == 1 ? 8 : (q == 2 ? 10 : (q == 3 ? 14 : 16))));
+}
+
+template <class S, int P, bool LO>
+__device__ __forceinline__ void xface_side(const LatParams &p, const StepParams &s, uint8_t *buf, uint32_t c, uint32_t m, uint32_t y,
+                                           uint32_t z, const S *out) {
+    using R = typename Pop<S>::real;
+    constexpr uint32_t SLOT = slot_bytes<S>();
+    const Consts<R> &k = K<R>(p);
+    const uint32_t b = LO ? m - 1 : m + 1;
+    const uint32_t cb = LO ? c - 1 : c + 1;
+    const uint32_t info = p.xface_info[LO ? 0 : 1];
+    R g[19];
+#pragma unroll
+    for (int i = 0; i < 19; i++) g[i] = Pop<S>::cvt(out[i]);
+    R fb[5];  // the face cell's inward populations
+    if ((info & 3u) == 2u) {
+        // free slip: the mirror image in x of m's populations
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            fb[q] = g[DIR(-CX(inward_dir(LO, q)), CY(inward_dir(LO, q)), CZ(inward_dir(LO, q)))];
+        }
+    } else {
+        const Moments<R> mo = moments<R>(g);
+        R rho = (R)1 + mo.rho1;
+        R ux = mo.jx / rho - (R)0.5 * k.grav[0];
+        R uy = mo.jy / rho - (R)0.5 * k.grav[1];
+        R uz = mo.jz / rho - (R)0.5 * k.grav[2];
+        R pi[6];
+        pi_neq<R>(mo, rho, ux, uy, uz, pi);
+        if ((info & 3u) == 0u) {
+            if (p.total_p) {
+                const R uinf2 = k.u_inf[0] * k.u_inf[0] + k.u_inf[1] * k.u_inf[1] + k.u_inf[2] * k.u_inf[2];
+                rho = ((R)(1.0 / 3.0) + (R)0.5 * uinf2) / ((R)(1.0 / 3.0) + (R)0.5 * (ux * ux + uy * uy + uz * uz));
+            } else {
+                ux = k.u_inf[0]; uy = k.u_inf[1]; uz = k.u_inf[2];
+            }
+        } else {
+            rho = 1;
+        }
+        const R rho1 = rho - (R)1;
+        const R usq = (R)1.5 * (ux * ux + uy * uy + uz * uz);
+        const R tr = (pi[0] + pi[1] + pi[2]) * (R)(1.0 / 3.0);
+#pragma unroll
+        for (int q = 0; q < 5; q++) fb[q] = feq_i<R>(inward_dir(LO, q), rho1, rho, ux, uy, uz, usq) + fneq_i<R>(inward_dir(LO, q), pi, tr);
+    }
+    Rng rng{sr_hash_mix(b, s.next_seed_mix)};
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+        const int i = inward_dir(LO, q);
+        // the target row must collide: not on a non-periodic y or z face
+        const int64_t ty = (int64_t)y + CY(i), tz = (int64_t)z + CZ(i);
+        if (!p.per[1] && (ty <= 0 || ty >= (int64_t)p.NY - 1)) continue;
+        if (!p.per[2] && (tz <= 0 || tz >= (int64_t)p.NZ - 1)) continue;
+        const S v = Pop<S>::enc(fb[q], rng);
+        const int j = P == 0 ? OPP(i) : i;
+        ((S *)(buf + j * SLOT))[lead<S, P>(j) + cb] = v;
+    }
+}
+
+// The x-face cell b next to cell m (b = m - 1 when x = 1, b = m + 1 when
+// x = NX - 2), on a planar x face whose inner neighbour is m: its populations
+// for the next step are what the face kernel of the next step would write
+// from m's post-collision state (shader.rs:630-687), so the thread that just
+// collided m computes them from its rounded outputs, with the face kernel's
+// arithmetic and random sequence, and writes them into b's slots of the
+// staged tile; they reach HBM with the tile.  Only the 5 directions entering
+// the domain are needed (the face kernel's store mask of a planar x face).
+template <class S, int P>
+__device__ __forceinline__ void xface_from_inner(const LatParams &p, const StepParams &s, uint8_t *buf, uint32_t c, uint32_t m, uint32_t x,
+                                                 uint32_t y, uint32_t z, const S *out) {
+    if (x == 1) xface_side<S, P, true>(p, s, buf, c, m, y, z, out);
+    else xface_side<S, P, false>(p, s, buf, c, m, y, z, out);
+}
+
 // A cell of a periodic-z boundary plane at input parity 1: the links that
 // leave the domain in z wrap to the other side, so those inputs and outputs go
 // straight to HBM; the others use the staged tile like every other cell.
 template <class S, int COLL>
-__device__ __noinline__ void zwrap_cell(const LatParams &p, const StepParams &s, uint8_t *buf, uint32_t c, uint32_t n, uint32_t x,
+__device__ __forceinline__ void zwrap_cell(const LatParams &p, const StepParams &s, uint8_t *buf, uint32_t c, uint32_t n, uint32_t x,
                                         uint32_t y, uint32_t z) {
     using R = typename Pop<S>::real;
     constexpr uint32_t SLOT = slot_bytes<S>();
@@ -398,16 +575,16 @@ __global__ void __launch_bounds__(BLOCK, sizeof(S) == 8 ? 2 : 3) k_bulk_tma(cons
     extern __shared__ __align__(128) uint8_t sm_raw[];
     // realigned with pointer arithmetic so the compiler keeps it a shared-memory pointer
     uint8_t *sm = sm_raw + ((128u - (smem_addr(sm_raw) & 127u)) & 127u);
-    __shared__ __align__(8) uint64_t full[2], empty[2];
+    __shared__ __align__(8) uint64_t full[NBUF], empty[NBUF];
     __shared__ int64_t tab_sh[19];  // plane shift (elements)
     __shared__ int tab_lead[19];    // plane lead (elements)
     const uint32_t ntiles = (p.N + T - 1) / T;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
-        mbar_init(&full[0], 1);
-        mbar_init(&full[1], 1);
-        mbar_init(&empty[0], CTHREADS);
-        mbar_init(&empty[1], CTHREADS);
+        for (int q = 0; q < NBUF; q++) {
+            mbar_init(&full[q], 1);
+            mbar_init(&empty[q], CTHREADS);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (threadIdx.x == 32) {
@@ -421,24 +598,24 @@ __global__ void __launch_bounds__(BLOCK, sizeof(S) == 8 ? 2 : 3) k_bulk_tma(cons
     S *pop = (S *)p.pop;
     if (warp == CWARPS) {
         // ------------------------------------------------ producer warp
-        // iteration it (0 .. K+1 for this block's K tiles): write back tile
-        // it-2 from buffer it&1 once the compute warps released it, then load
-        // tile it into the same buffer
+        // iteration it (0 .. K+NBUF-1 for this block's K tiles): write back
+        // tile it-NBUF from buffer it%NBUF once the compute warps released
+        // it, then load tile it into the same buffer
         const int64_t N = p.N;
         const uint32_t G = gridDim.x;
         const uint32_t K = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / G + 1 : 0;
         uint32_t it = 0;
         bool alive = true;
-        for (; it < K + 2; ++it) {
-            const int b = it & 1;
-            if (it >= 2) {
-                if (!mbar_wait_bounded(&empty[b], ((it - 2) >> 1) & 1)) { alive = false; break; }
+        for (; it < K + NBUF; ++it) {
+            const int b = it % NBUF;
+            if (it >= NBUF) {
+                if (!mbar_wait_bounded(&empty[b], ((it - NBUF) / NBUF) & 1)) { alive = false; break; }
                 if (lane < 19) {
                     // plane j's slots of the tile's cells back to HBM: cells
                     // and slots clamped to [0, N); the 16-byte-aligned interior
                     // with one bulk store, the ragged ends with plain stores
                     const int j = lane;
-                    const uint32_t n0 = (blockIdx.x + (it - 2) * G) * T;
+                    const uint32_t n0 = (blockIdx.x + (it - NBUF) * G) * T;
                     const int64_t sh = tab_sh[j];
                     const int64_t lo = max((int64_t)n0, -sh);
                     int64_t hi = min(min((int64_t)n0 + (int64_t)T, N), N - sh);
@@ -464,11 +641,11 @@ __global__ void __launch_bounds__(BLOCK, sizeof(S) == 8 ? 2 : 3) k_bulk_tma(cons
         if (!alive && lane == 0) {
             atomicOr(p.err, ERR_COPY_WAIT);
             // drain the loads still in flight (the last one into each buffer)
-            for (int bq = 0; bq < 2; bq++) {
+            for (int bq = 0; bq < NBUF; bq++) {
                 int last = -1;
                 for (uint32_t q = 0; q < min(it, K); q++)
-                    if ((int)(q & 1) == bq) last = (int)q;
-                if (last >= 0) mbar_wait_bounded(&full[bq], ((uint32_t)last >> 1) & 1);
+                    if ((int)(q % NBUF) == bq) last = (int)q;
+                if (last >= 0) mbar_wait_bounded(&full[bq], ((uint32_t)last / NBUF) & 1);
             }
         }
         if (lane < 19) bulk_wait_all();
@@ -479,8 +656,8 @@ __global__ void __launch_bounds__(BLOCK, sizeof(S) == 8 ? 2 : 3) k_bulk_tma(cons
     const bool zper = p.per[2] != 0;
     uint32_t it = 0;
     for (uint32_t t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
-        const int b = it & 1;
-        if (!mbar_wait_bounded(&full[b], (it >> 1) & 1)) {
+        const int b = it % NBUF;
+        if (!mbar_wait_bounded(&full[b], (it / NBUF) & 1)) {
             atomicOr(p.err, ERR_COPY_WAIT);
             return;
         }
@@ -491,7 +668,8 @@ __global__ void __launch_bounds__(BLOCK, sizeof(S) == 8 ? 2 : 3) k_bulk_tma(cons
         for (uint32_t c = threadIdx.x; c < T; c += CTHREADS) {
             const uint32_t n = n0 + c;
             if (n >= p.N) break;
-            if (fl[c] != 0u) continue;
+            const uint32_t fg = fl[c];
+            if ((fg & ~FLAG_XFACE) != 0u) continue;
             uint32_t x, y, z;
             coords(p, n, x, y, z);
             if (P == 1 && zper && (z == 0 || z == p.NZ - 1)) {
@@ -532,6 +710,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(S) == 8 ? 2 : 3) k_bulk_tma(cons
                 const int j = (P == 0) ? OPP(i) : i;  // plane receiving output f[i]
                 ((S *)(buf + j * SLOT))[lead<S, P>(j) + c] = out[i];
             }
+            if (fg & FLAG_XFACE) xface_from_inner<S, P>(p, s, buf, c, n, x, y, z, out);
         }
         fence_async_smem();  // this thread's shared-memory writes, before the bulk stores read them
         mbar_arrive(&empty[b]);
@@ -658,94 +837,6 @@ __global__ void __launch_bounds__(BLOCK) k_walls(const __grid_constant__ LatPara
     if (threadIdx.x == 0) *p.ticket = 0u;
 }
 
-// ---------------------------------------------------------------- faces
-template <class R, int M, int I>
-__device__ __forceinline__ void mirror_one(const R *g, R *f) {
-    constexpr int j = DIR((M & 1) ? -CX(I) : CX(I), (M & 2) ? -CY(I) : CY(I), (M & 4) ? -CZ(I) : CZ(I));
-    f[I] = g[j];
-}
-template <class R, int M, int... Is>
-__device__ __forceinline__ void mirror_all(const R *g, R *f, std::integer_sequence<int, Is...>) {
-    (mirror_one<R, M, Is>(g, f), ...);
-}
-template <class R, int M>
-__device__ __forceinline__ void mirror(const R *g, R *f) {
-    mirror_all<R, M>(g, f, std::make_integer_sequence<int, 19>{});
-}
-
-template <class S, int P>
-__global__ void __launch_bounds__(BLOCK) k_faces(const __grid_constant__ LatParams p, const __grid_constant__ StepParams s) {
-    using R = typename Pop<S>::real;
-    constexpr int Q = 1 - P;
-    const Consts<R> &k = K<R>(p);
-    const uint32_t kf = blockIdx.x * BLOCK + threadIdx.x;
-    if (kf >= p.nface) return;
-    const uint32_t b = p.faces[kf];
-    const uint32_t info = p.face_info[kf];
-    uint32_t x, y, z;
-    coords(p, b, x, y, z);
-    uint32_t cx = x, cy = y, cz = z;
-    if (!p.per[0]) cx = min(max(cx, 1u), p.NX - 2);
-    if (!p.per[1]) cy = min(max(cy, 1u), p.NY - 2);
-    if (!p.per[2]) cz = min(max(cz, 1u), p.NZ - 2);
-    const uint32_t m = (cz * p.NY + cy) * p.NX + cx;
-    const uint32_t fg = p.flags[m];
-    const Nb nbm = make_nb(p, cx, cy, cz);
-    R f[19];
-    if ((info & 3u) == 2u) {
-        // free slip: mirror image of the inner neighbour (no reference counterpart)
-        if ((fg & 3u) == 0u) {
-            R g[19];
-            load_prev_out<S, Q>(p, m, nbm, g);
-            switch ((info >> 2) & 7u) {
-                case 1: mirror<R, 1>(g, f); break;
-                case 2: mirror<R, 2>(g, f); break;
-                case 3: mirror<R, 3>(g, f); break;
-                case 4: mirror<R, 4>(g, f); break;
-                case 5: mirror<R, 5>(g, f); break;
-                case 6: mirror<R, 6>(g, f); break;
-                case 7: mirror<R, 7>(g, f); break;
-                default: mirror<R, 0>(g, f); break;
-            }
-        } else {
-            const R usq = (R)1.5 * (k.u_inf[0] * k.u_inf[0] + k.u_inf[1] * k.u_inf[1] + k.u_inf[2] * k.u_inf[2]);
-#pragma unroll
-            for (int i = 0; i < 19; i++) f[i] = feq_i<R>(i, (R)0, (R)1, k.u_inf[0], k.u_inf[1], k.u_inf[2], usq);
-        }
-    } else {
-        R rho = 1, ux = k.u_inf[0], uy = k.u_inf[1], uz = k.u_inf[2];
-        R pi[6] = {0, 0, 0, 0, 0, 0};
-        if ((fg & 3u) == 0u) {
-            R g[19];
-            load_prev_out<S, Q>(p, m, nbm, g);
-            const Moments<R> mo = moments<R>(g);
-            rho = (R)1 + mo.rho1;
-            ux = mo.jx / rho - (R)0.5 * k.grav[0];
-            uy = mo.jy / rho - (R)0.5 * k.grav[1];
-            uz = mo.jz / rho - (R)0.5 * k.grav[2];
-            pi_neq<R>(mo, rho, ux, uy, uz, pi);
-        }
-        if ((info & 3u) == 0u) {
-            if (p.total_p) {
-                const R uinf2 = k.u_inf[0] * k.u_inf[0] + k.u_inf[1] * k.u_inf[1] + k.u_inf[2] * k.u_inf[2];
-                rho = ((R)(1.0 / 3.0) + (R)0.5 * uinf2) / ((R)(1.0 / 3.0) + (R)0.5 * (ux * ux + uy * uy + uz * uz));
-            } else {
-                ux = k.u_inf[0]; uy = k.u_inf[1]; uz = k.u_inf[2];
-            }
-        } else {
-            rho = 1;
-        }
-        const R rho1 = rho - (R)1;
-        const R usq = (R)1.5 * (ux * ux + uy * uy + uz * uz);
-        const R tr = (pi[0] + pi[1] + pi[2]) * (R)(1.0 / 3.0);
-#pragma unroll
-        for (int i = 0; i < 19; i++) f[i] = feq_i<R>(i, rho1, rho, ux, uy, uz, usq) + fneq_i<R>(i, pi, tr);
-    }
-    const Nb nbb = make_nb(p, x, y, z);
-    Rng rng{sr_hash_mix(b, s.seed_mix)};
-    store_prev_out<S, Q>(p, b, nbb, info >> 8, f, rng);
-}
-
 // ---------------------------------------------------------------- init
 // shader.rs:623-628: every cell holds the equilibrium at u_init (step seed 0)
 template <class S>
@@ -769,7 +860,7 @@ __global__ void __launch_bounds__(BLOCK) k_dump(const __grid_constant__ LatParam
     const Consts<R> &k = K<R>(p);
     const uint32_t n = blockIdx.x * BLOCK + threadIdx.x;
     if (n >= p.N) return;
-    const uint32_t fg = p.flags[n];
+    const uint32_t fg = p.flags[n] & ~FLAG_XFACE;
     if (fg & 3u) { p.dump[n] = make_float4(__int_as_float(0x7fc00000), __int_as_float(0x7fc00000), __int_as_float(0x7fc00000), __int_as_float(0x7fc00000)); return; }
     const uint32_t rec = fg >> 2;
     if (rec) {
@@ -796,7 +887,7 @@ template <class S, int Q>
 __device__ __forceinline__ bool cell_macro(const LatParams &p, uint32_t m, float &rho, float &ux, float &uy, float &uz) {
     using R = typename Pop<S>::real;
     const Consts<R> &k = K<R>(p);
-    const uint32_t fg = p.flags[m];
+    const uint32_t fg = p.flags[m] & ~FLAG_XFACE;
     if (fg & 3u) return false;
     const uint32_t rec = fg >> 2;
     if (rec) {
@@ -949,14 +1040,14 @@ template <class S, int P, int COLL>
 static cudaError_t step_t(const LatParams &p, const StepParams &s, cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join,
                           cudaEvent_t *ev) {
     if (ev) cudaEventRecord(ev[0], st);
-    const bool overlap = side && p.nrec && p.nface;
+    const bool overlap = side && p.nrec && s.nface;
     if (overlap) {
         cudaEventRecord(fork, st);
         cudaStreamWaitEvent(side, fork, 0);
         k_walls<S, P, COLL><<<blocks_for(p.nrec), BLOCK, 0, side>>>(p, s);
         cudaEventRecord(join, side);
     }
-    if (p.nface) k_faces<S, P><<<blocks_for(p.nface), BLOCK, 0, st>>>(p, s);
+    if (s.nface) k_faces<S, P><<<blocks_for(s.nface), BLOCK, 0, st>>>(p, s);
     if (ev) cudaEventRecord(ev[1], st);
     if (overlap) cudaStreamWaitEvent(st, join, 0);
     else if (p.nrec) k_walls<S, P, COLL><<<blocks_for(p.nrec), BLOCK, 0, st>>>(p, s);

@@ -87,6 +87,9 @@ struct lbm_lattice {
     std::vector<cudaEvent_t> prof_ev;
     uint64_t prof_steps = 0;
     uint64_t pop_bytes = 0;
+    uint32_t nface_rest = 0;   // face cells the face kernel handles once x faces are fused
+    bool xfuse = false;        // planar x faces are written by the staged kernel
+    bool fused_valid = false;  // the last step wrote the fused x faces for the next one
     uint32_t *err_host = nullptr;  // pinned
 
     void *dalloc(size_t bytes) {
@@ -183,6 +186,8 @@ lbm::StepParams step_params(const lbm_lattice *h, const lbm_step_in &s, uint32_t
     lbm::StepParams sp{};
     sp.seed = (uint32_t)step_index * 2654435761u;  // lattice.rs:676
     sp.seed_mix = sp.seed * 0x85EBCA77u + 0x632BE5ABu;
+    sp.next_seed_mix = ((uint32_t)(step_index + 1) * 2654435761u) * 0x85EBCA77u + 0x632BE5ABu;
+    sp.nface = h->fused_valid ? h->nface_rest : h->nface;
     sp.slot = slot;
     for (int a = 0; a < 3; a++) {
         sp.omega[a] = (float)s.omega[a];
@@ -274,17 +279,6 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
             if (edge) { for (uint64_t x = 0; x < NX; x++) visit(x); }
             else { visit(0); visit(NX - 1); }
         }
-    // face cells are independent; grouping them by kind and store mask keeps
-    // each warp on one code path
-    {
-        std::vector<size_t> ord(faces.size());
-        for (size_t k = 0; k < ord.size(); k++) ord[k] = k;
-        std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) { return finfo[a] < finfo[b]; });
-        std::vector<uint32_t> f2(faces.size()), i2(faces.size());
-        for (size_t k = 0; k < ord.size(); k++) { f2[k] = faces[ord[k]]; i2[k] = finfo[ord[k]]; }
-        faces.swap(f2);
-        finfo.swap(i2);
-    }
     h->nface = (uint32_t)faces.size();
 
     // wall records (lattice.rs:454-482; record_words 202-218)
@@ -335,6 +329,50 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
             uint32_t c = geom->walls[r].cell;
             if ((flags[c] & 3u) == 0) flags[c] = (uint32_t)(r + 1) << 2;  // a later record of the same cell wins
         }
+    }
+
+    // Planar x-face cells (x = 0 or NX - 1, y and z inside) whose inner
+    // neighbour m = b +- 1 is a plain fluid cell are written by the staged
+    // kernel while it collides m (flag bit FLAG_XFACE on m), one step ahead;
+    // only the first step after setup or a state load needs the face kernel
+    // for them.  They go to the end of the face list.
+    const bool tma_ok = (NX * storage_bytes(st.storage)) % 16 == 0 && !per[0] && !per[1];
+    std::vector<char> fused(faces.size(), 0);
+    uint32_t xinfo[2] = {0, 0};
+    if (tma_ok && !(std::getenv("SIMLAB_LBM_NO_TMA") && std::getenv("SIMLAB_LBM_NO_TMA")[0] == '1')) {
+        for (size_t k = 0; k < faces.size(); k++) {
+            const uint64_t c = faces[k], x = c % NX, y = (c / NX) % NY, z = c / (NX * NY);
+            if (x != 0 && x != NX - 1) continue;
+            // rows away from the y and z boundaries (periodic or not), so the
+            // slots written stay inside the tile's linear slot range
+            if (y == 0 || y == NY - 1 || z == 0 || z == NZ - 1) continue;
+            const uint64_t m = x == 0 ? c + 1 : c - 1;
+            if (flags[m] != 0) continue;
+            fused[k] = 1;
+            flags[m] |= lbm::FLAG_XFACE;
+            xinfo[x == 0 ? 0 : 1] = finfo[k] & 0xffu;
+        }
+    }
+    {
+        // face cells are independent; grouping them by kind and store mask
+        // keeps each warp on one code path
+        std::vector<size_t> ord(faces.size());
+        for (size_t k = 0; k < ord.size(); k++) ord[k] = k;
+        std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) {
+            if (fused[a] != fused[b]) return fused[a] < fused[b];
+            return finfo[a] < finfo[b];
+        });
+        std::vector<uint32_t> f2(faces.size()), i2(faces.size());
+        uint32_t rest = 0;
+        for (size_t k = 0; k < ord.size(); k++) {
+            f2[k] = faces[ord[k]];
+            i2[k] = finfo[ord[k]];
+            rest += fused[ord[k]] ? 0u : 1u;
+        }
+        faces.swap(f2);
+        finfo.swap(i2);
+        h->nface_rest = rest;
+        h->xfuse = rest < faces.size();
     }
 
     // probes
@@ -414,6 +452,8 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     p.moving = 0;
     fill_consts<float>(p.kf, st);
     fill_consts<double>(p.kd, st);
+    p.xface_info[0] = xinfo[0];
+    p.xface_info[1] = xinfo[1];
     // sponge ramps per axis (shader.rs:528-538): 1 - p / width inside a layer
     std::vector<float> tabf;
     std::vector<double> tabd;
@@ -503,6 +543,7 @@ void run_impl(lbm_lattice *h, const lbm_step_in *steps, uint64_t n, double *forc
                                       h->nslices, h->npix, h->sacc, h->stream),
                    "sample kernels");
             h->steps_done++;
+            h->fused_valid = h->xfuse;
         }
         if (readback) {
             ck(cudaMemcpyAsync(h->hist_host, p.hist, len * 8 * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "history readback");
@@ -704,7 +745,7 @@ int lbm_mass(lbm_lattice *h, double *mass, uint64_t *nonfinite) {
 }
 
 // checkpoint blob: header, populations, records (u32), records (f64, FP64 only)
-struct StateHeader { uint64_t magic, cells, steps_done, nrec; int32_t storage, collision; };
+struct StateHeader { uint64_t magic, cells, steps_done, nrec; int32_t storage, collision, fused_valid, _pad; };
 static const uint64_t STATE_MAGIC = 0x4c424d5354415431ull;
 
 int lbm_state_size(const lbm_lattice *h, uint64_t *bytes) {
@@ -720,7 +761,7 @@ int lbm_save_state(lbm_lattice *h, void *buf, uint64_t bytes) {
         uint64_t need;
         lbm_state_size(h, &need);
         if (bytes < need) throw LbmError(LBM_ERR_INVALID, "state buffer too small");
-        StateHeader hd{STATE_MAGIC, h->lp.N, h->steps_done, h->nrec, h->setup.storage, h->setup.collision};
+        StateHeader hd{STATE_MAGIC, h->lp.N, h->steps_done, h->nrec, h->setup.storage, h->setup.collision, h->fused_valid ? 1 : 0, 0};
         char *o = (char *)buf;
         std::memcpy(o, &hd, sizeof hd);
         o += sizeof hd;
@@ -753,6 +794,8 @@ int lbm_load_state(lbm_lattice *h, const void *buf, uint64_t bytes) {
         if (h->lp.recd && h->nrec) ck(cudaMemcpyAsync(h->lp.recd, o, (size_t)h->nrec * lbm::RD * 8, cudaMemcpyHostToDevice, h->stream), "state upload");
         h->wait();
         h->steps_done = hd.steps_done;
+        // the blob holds the fused x faces' slots when its step wrote them
+        h->fused_valid = h->xfuse && hd.fused_valid != 0;
     });
 }
 

@@ -49,6 +49,8 @@ constexpr uint32_t RS = 40, R_MASK = 0, R_CELL = 1, R_Q = 2, R_FPOST = 11, R_MAC
 constexpr uint32_t RD = 28, RD_FPOST = 0, RD_MACRO = 18, RD_FT = 22;
 
 constexpr int BLOCK = 256;
+// flag bit of a fluid cell whose x neighbour is a planar x-face cell it feeds
+constexpr uint32_t FLAG_XFACE = 0x80000000u;
 constexpr uint32_t PLANE_ALIGN = 256;  // cells
 
 // error bits set by kernels (read by the host after each chunk)
@@ -109,6 +111,7 @@ struct LatParams {
     uint32_t sp_w[6];          // sponge widths in cells, -x,+x,-y,+y,-z,+z
     const float *sp_tab;       // sponge ramp per x, then per y, then per z (NX + NY + NZ values)
     const double *sp_tabd;     // the same in FP64
+    uint32_t xface_info[2];    // face info (kind | mirror << 2) of the -x and +x faces, for fused x faces
     int tma;                   // the staged bulk kernel applies (NX * element size % 16 == 0)
     Consts<float> kf;
     Consts<double> kd;
@@ -117,6 +120,8 @@ struct LatParams {
 struct StepParams {
     uint32_t seed;   // stochastic rounding seed of this step (lattice.rs:676)
     uint32_t seed_mix;  // seed * 0x85EBCA77 + 0x632BE5AB, the seed's term of sr_hash
+    uint32_t next_seed_mix;  // the same for the next step
+    uint32_t nface;          // face cells the face kernel handles this step
     uint32_t slot;   // history slot of this step
     float omega[3];  // angular velocity, rad per step
     double omega_d[3];
