@@ -252,6 +252,25 @@ void lbm_voxels_free(lbm_voxels *v);
 int lbm_inside_grid(const double *verts, uint64_t nverts, const uint32_t *tris, uint64_t ntris,
                     const double origin[3], double h, const uint32_t dims[3], uint8_t *out);
 
+/* Allocation-free force and moment sum over wall records (no counterpart in
+ * the reference).  For callers that cannot allocate device memory where they
+ * need the sum: code running during CUDA graph capture, hosts whose device
+ * memory comes from their own pool allocator, embedded callers with a fixed
+ * footprint.  records_dev: nrec records of 40 u32 words in device memory
+ * (the layout of lbm_records); forces_dev: 6 doubles in device memory
+ * (force, then moment); stream: a cudaStream_t (NULL for the default
+ * stream).  The call enqueues the work and returns; it allocates and frees
+ * nothing.  Scratch: a fixed array inside this library, 256 KiB on every
+ * device that loads it, kept until the process exits and shared by all calls
+ * on that device: calls whose work overlaps on the GPU race and must be
+ * ordered by the caller.  At most lbm_record_forces_noalloc_max() records
+ * (1,048,576); more is rejected with LBM_ERR_INVALID.  The first call on a
+ * device looks up the scratch address and should come before any stream
+ * capture.  Errors: message from lbm_noalloc_error. */
+int lbm_record_forces_noalloc(const uint32_t *records_dev, uint64_t nrec, double *forces_dev, void *stream);
+uint64_t lbm_record_forces_noalloc_max(void);
+int lbm_noalloc_error(char *buf, uint64_t len);
+
 #ifdef __cplusplus
 }
 #endif

@@ -175,6 +175,9 @@ def library() -> C.CDLL:
     L.lbm_voxels_free.argtypes = [vp]
     L.lbm_voxels_free.restype = None
     L.lbm_inside_grid.argtypes = [dp, u64, C.POINTER(C.c_uint32), u64, dp, C.c_double, C.POINTER(C.c_uint32), C.POINTER(C.c_uint8)]
+    L.lbm_record_forces_noalloc.argtypes = [vp, u64, vp, vp]
+    L.lbm_record_forces_noalloc_max.restype = u64
+    L.lbm_noalloc_error.argtypes = [C.c_char_p, u64]
     _lib_handle = L
     return L
 
@@ -550,6 +553,18 @@ def inside_grid(verts, tris, origin: Sequence[float], h: float, dims: Sequence[i
     if rc != 0:
         raise _global_error(rc)
     return out.astype(bool)
+
+
+def record_forces_noalloc(records_dev_ptr: int, nrec: int, forces_dev_ptr: int, stream: int = 0) -> None:
+    """Force and moment sum over wall records already in device memory, into
+    6 doubles in device memory, without allocating anything (enqueued on
+    `stream`; see lbm_record_forces_noalloc in include/simlab_lbm.h)."""
+    L = library()
+    rc = L.lbm_record_forces_noalloc(C.c_void_p(records_dev_ptr), int(nrec), C.c_void_p(forces_dev_ptr), C.c_void_p(stream or None))
+    if rc != 0:
+        buf = C.create_string_buffer(512)
+        L.lbm_noalloc_error(buf, 512)
+        raise LbmError(rc, buf.value.decode(errors="replace"))
 
 
 def halfway(vox: StaticVoxels) -> StaticVoxels:
