@@ -51,7 +51,7 @@ def peaks():
 
 def traffic_from_profile(storage_name: str):
     """DRAM bytes per k_bulk launch from the committed ncu summary, if any."""
-    f = ROOT / "profiles" / f"k_bulk_{storage_name}_arm_512x256x256.md"
+    f = ROOT / "profiles" / f"k_bulk_tma_{storage_name}_arm_512x256x256.md"
     if not f.exists():
         return None
     m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", f.read_text())
