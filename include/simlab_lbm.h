@@ -252,6 +252,90 @@ void lbm_voxels_free(lbm_voxels *v);
 int lbm_inside_grid(const double *verts, uint64_t nverts, const uint32_t *tris, uint64_t ntris,
                     const double origin[3], double h, const uint32_t dims[3], uint8_t *out);
 
+/* ------------------------------------------------------------------------
+ * Multi-level D3Q27 lattice: `MultiLattice` of crates/cfd/src/mlattice.rs
+ * with the collision of crates/cfd/src/mshader.rs.  Pull streaming over two
+ * population sets per level, the cumulant-type collision (deviatoric second
+ * moments relaxed with the viscous rate, every higher cumulant to
+ * equilibrium), Bouzidi walls with momentum exchange on the finest level,
+ * nested node-aligned boxes of half the cell size stepped twice per parent
+ * step.  Faces of type FREE_SLIP are not available here (LBM_ERR_UNSUPPORTED).
+ * ------------------------------------------------------------------------ */
+
+/* `LevelBox` (mlattice.rs:15-21): lo is the parent node of the level's node
+ * 0, n the number of parent nodes it spans per axis (dims = 2 (n - 1) + 1). */
+typedef struct {
+    int32_t lo[3];
+    uint32_t n[3];
+} lbm_level_box;
+
+/* `MultiSetup` (mlattice.rs:23-47), field for field. */
+typedef struct {
+    uint32_t dims0[3];          /* coarsest level size, cells */
+    uint32_t nboxes;            /* number of refinement boxes (levels - 1) */
+    const lbm_level_box *boxes; /* boxes of levels 1.., each in its parent's node coordinates */
+    int32_t faces[6];           /* lbm_face_bc: VELOCITY, OPEN or PERIODIC (periodic only without boxes) */
+    double nu0;                 /* lattice viscosity on the coarsest level (doubles per finer level) */
+    double smagorinsky;
+    double u_inf[3];
+    double u_init[3];
+    double body_force0[3];      /* acceleration on the coarsest level (halves per finer level) */
+    uint32_t sponge[6];         /* sponge widths on the coarsest level, cells */
+    double sponge_tau;
+    double sponge_sigma;
+    int32_t absorb_velocity;
+    int32_t total_pressure_inlet;
+    int32_t storage;            /* lbm_storage */
+    int32_t debug_dump;
+    double center[3];           /* moment reference, finest-level coordinates */
+} lbm_multi_setup;
+
+typedef struct lbm_multi lbm_multi;
+
+/* MultiLattice::new (mlattice.rs:195-688).  Geometry (kind 0 or 1) is in the
+ * finest level's cell indices; wall records use D3Q27 directions
+ * (i = (cx+1) + 3 (cy+1) + 9 (cz+1)).  Same validation messages as the
+ * reference ("refinement box 1 does not fit inside its parent", "periodic
+ * faces only work without refinement", ...).  probes may be NULL. */
+int lbm_create_multi(const lbm_multi_setup *setup, const lbm_geometry *geom, const lbm_probes *probes, lbm_multi **out);
+void lbm_multi_destroy(lbm_multi *h);
+int lbm_multi_last_error(const lbm_multi *h, char *buf, uint64_t len);
+
+/* sub_steps / level_dims / level_cells (mlattice.rs:705-721).  levels: the
+ * number of levels; dims: 3 per level; cells: 1 per level. */
+int lbm_multi_levels(const lbm_multi *h, uint32_t *levels);
+int lbm_multi_sub_steps(const lbm_multi *h, uint32_t *sub_steps);
+int lbm_multi_level_dims(const lbm_multi *h, uint32_t *dims);
+int lbm_multi_level_cells(const lbm_multi *h, uint64_t *cells);
+
+/* MultiLattice::run (mlattice.rs:723-784): n finest steps, a multiple of
+ * sub_steps; forces_out: 6 doubles per finest step (force and moment about
+ * center on the geometry, finest lattice units). */
+int lbm_multi_run(lbm_multi *h, const lbm_step_in *steps, uint64_t n, double *forces_out);
+
+/* n finest still steps (a multiple of sub_steps) enqueued without waiting
+ * (for timing; no reference counterpart). */
+int lbm_multi_advance(lbm_multi *h, uint64_t n);
+int lbm_multi_stream(lbm_multi *h, void **stream);
+int lbm_multi_synchronize(lbm_multi *h);
+int lbm_multi_set_timeout(lbm_multi *h, double seconds);
+
+/* MultiLattice::macros (mlattice.rs:883-901): (rho, ux, uy, uz) per cell of
+ * one level, NaN except plain fluid cells; needs debug_dump. */
+int lbm_multi_macros(lbm_multi *h, uint32_t level, float *out);
+
+/* MultiLattice::records (mlattice.rs:903-905): 24 u32 words per record
+ * (mask, cell, q as 13 f16 pairs in slot order, force, moment, 3 zero). */
+int lbm_multi_records(lbm_multi *h, uint32_t *out, uint64_t cap_words);
+
+/* steps_done counts finest steps; nrec, memory_bytes, storage as lbm_info;
+ * cells = the sum of the levels' cells. */
+int lbm_multi_get_info(const lbm_multi *h, lbm_info *out);
+
+/* FP64 mass and non-finite count over the plain fluid cells of one level
+ * (no reference counterpart). */
+int lbm_multi_mass(lbm_multi *h, uint32_t level, double *mass, uint64_t *nonfinite);
+
 /* Allocation-free force and moment sum over wall records (no counterpart in
  * the reference).  For callers that cannot allocate device memory where they
  * need the sum: code running during CUDA graph capture, hosts whose device

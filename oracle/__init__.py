@@ -141,3 +141,101 @@ class OracleLattice:
         out = np.zeros(19 * self.setup.cells(), dtype=np.float64)
         self._L.orc_raw(self._h, out.ctypes.data)
         return out.reshape(19, -1)
+
+
+class OracleMulti:
+    """The multi-level D3Q27 oracle with the readback of simlab_b200.MultiLattice.
+
+    real64=False: the reference's FP32 update; real64=True: the FP64 oracle."""
+
+    def __init__(self, setup, geometry=None, real64: bool = False):
+        from simlab_b200.lbm import geometry_struct
+
+        L = library()
+        vp, u64 = C.c_void_p, C.c_ulonglong
+        L.m27_create.argtypes = [vp, vp, C.c_int]
+        L.m27_create.restype = vp
+        L.m27_destroy.argtypes = [vp]
+        L.m27_destroy.restype = None
+        L.m27_run.argtypes = [vp, vp, u64, vp]
+        L.m27_levels.argtypes = [vp]
+        L.m27_levels.restype = C.c_uint
+        L.m27_dims.argtypes = [vp, vp]
+        L.m27_macros.argtypes = [vp, C.c_uint, vp]
+        L.m27_nrec.argtypes = [vp]
+        L.m27_nrec.restype = u64
+        L.m27_records.argtypes = [vp, vp]
+        L.m27_flags.argtypes = [vp, C.c_uint, vp]
+        L.m27_fine_steps.argtypes = [vp]
+        L.m27_fine_steps.restype = u64
+        self._L = L
+        self.setup = setup
+        cs, keep = setup.to_c()
+        g, keep2 = geometry_struct(geometry)
+        h = L.m27_create(C.addressof(cs), C.addressof(g), int(real64))
+        del keep, keep2
+        if not h:
+            buf = C.create_string_buffer(1024)
+            L.orc_last_error(buf, 1024)
+            raise RuntimeError(buf.value.decode())
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.m27_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def levels(self) -> int:
+        return int(self._L.m27_levels(self._h))
+
+    def level_dims(self) -> list:
+        n = self.levels()
+        out = np.zeros(3 * n, dtype=np.uint32)
+        self._L.m27_dims(self._h, out.ctypes.data)
+        return [tuple(int(v) for v in out[3 * l:3 * l + 3]) for l in range(n)]
+
+    def sub_steps(self) -> int:
+        return 1 << (self.levels() - 1)
+
+    @property
+    def nrec(self) -> int:
+        return int(self._L.m27_nrec(self._h))
+
+    @property
+    def fine_steps(self) -> int:
+        return int(self._L.m27_fine_steps(self._h))
+
+    def run(self, fine) -> np.ndarray:
+        from simlab_b200.lbm import STEP_DTYPE, steps_array
+
+        a = fine if isinstance(fine, np.ndarray) and fine.dtype == STEP_DTYPE else steps_array(fine)
+        a = np.ascontiguousarray(a)
+        out = np.zeros((len(a), 6), dtype=np.float64)
+        if self._L.m27_run(self._h, a.ctypes.data, len(a), out.ctypes.data) != 0:
+            buf = C.create_string_buffer(1024)
+            self._L.orc_last_error(buf, 1024)
+            raise RuntimeError(buf.value.decode())
+        return out
+
+    def macros(self, level: int) -> np.ndarray:
+        d = self.level_dims()[level]
+        out = np.empty((d[0] * d[1] * d[2], 4), dtype=np.float32)
+        self._L.m27_macros(self._h, int(level), out.ctypes.data)
+        return out
+
+    def records(self) -> np.ndarray:
+        out = np.zeros(max(self.nrec, 1) * 24, dtype=np.uint32)
+        self._L.m27_records(self._h, out.ctypes.data)
+        return out
+
+    def flags(self, level: int) -> np.ndarray:
+        d = self.level_dims()[level]
+        out = np.zeros(d[0] * d[1] * d[2], dtype=np.uint32)
+        self._L.m27_flags(self._h, int(level), out.ctypes.data)
+        return out

@@ -7,6 +7,7 @@
 #include <string>
 
 #include "d3q19_oracle.hpp"
+#include "d3q27_oracle.hpp"
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -20,6 +21,20 @@ struct Handle {
     oracle::D3Q19<float> *f32 = nullptr;
     oracle::D3Q19<double> *f64 = nullptr;
 };
+}  // namespace
+
+// ---------------------------------------------------------------- D3Q27 levels
+namespace {
+struct Multi {
+    int real64;
+    oracle::Multi27<float> *f32 = nullptr;
+    oracle::Multi27<double> *f64 = nullptr;
+};
+template <class Fn>
+auto with(void *hp, Fn fn) {
+    Multi *h = (Multi *)hp;
+    return h->real64 ? fn(*h->f64) : fn(*h->f32);
+}
 }  // namespace
 
 extern "C" {
@@ -131,5 +146,69 @@ float orc_f16_to_f32(uint16_t h) { return oracle::f16_to_f32(h); }
 uint16_t orc_f16_bits_ref(float x) { return oracle::f16_bits_ref(x); }
 uint16_t orc_f32_to_bf16(float x) { return oracle::f32_to_bf16(x); }
 float orc_sround16(float x, uint32_t key, uint32_t seed) { return oracle::sround16(x, key, seed); }
+
+
+void *m27_create(const lbm_multi_setup *st, const lbm_geometry *geom, int real64) {
+    Multi *h = new Multi();
+    h->real64 = real64;
+    try {
+        if (real64) { h->f64 = new oracle::Multi27<double>(); h->f64->create(*st, geom); }
+        else { h->f32 = new oracle::Multi27<float>(); h->f32->create(*st, geom); }
+        return h;
+    } catch (const std::exception &e) {
+        g_err = e.what();
+        delete h->f32;
+        delete h->f64;
+        delete h;
+        return nullptr;
+    }
+}
+
+void m27_destroy(void *hp) {
+    Multi *h = (Multi *)hp;
+    if (!h) return;
+    delete h->f32;
+    delete h->f64;
+    delete h;
+}
+
+int m27_run(void *hp, const lbm_step_in *steps, unsigned long long n, double *forces) {
+    try {
+        return with(hp, [&](auto &m) {
+            auto out = m.run(steps, (size_t)n);
+            if (forces)
+                for (size_t k = 0; k < out.size(); k++) std::memcpy(forces + 6 * k, out[k].data(), 6 * sizeof(double));
+            return 0;
+        });
+    } catch (const std::exception &e) {
+        g_err = e.what();
+        return -1;
+    }
+}
+
+unsigned m27_levels(void *hp) { return with(hp, [](auto &m) { return (unsigned)m.levels(); }); }
+
+int m27_dims(void *hp, uint32_t *out) {
+    return with(hp, [&](auto &m) {
+        for (size_t l = 0; l < m.lv.size(); l++) { out[3 * l] = m.lv[l].NX; out[3 * l + 1] = m.lv[l].NY; out[3 * l + 2] = m.lv[l].NZ; }
+        return 0;
+    });
+}
+
+int m27_macros(void *hp, unsigned level, float *out) {
+    return with(hp, [&](auto &m) { m.macros(level, out); return 0; });
+}
+
+unsigned long long m27_nrec(void *hp) { return with(hp, [](auto &m) { return (unsigned long long)m.nrec; }); }
+
+int m27_records(void *hp, uint32_t *out) {
+    return with(hp, [&](auto &m) { std::memcpy(out, m.rec_words.data(), m.rec_words.size() * 4); return 0; });
+}
+
+int m27_flags(void *hp, unsigned level, uint32_t *out) {
+    return with(hp, [&](auto &m) { std::memcpy(out, m.lv[level].flags.data(), m.lv[level].flags.size() * 4); return 0; });
+}
+
+unsigned long long m27_fine_steps(void *hp) { return with(hp, [](auto &m) { return (unsigned long long)m.fine_steps; }); }
 
 }  // extern "C"

@@ -1,0 +1,83 @@
+// Launch parameters and launchers of the multi-level D3Q27 time step
+// (d3q27_kernels.cu), shared with the host driver (mlattice.cu).
+//
+// Reference semantics: crates/cfd/src/mshader.rs (velocity set and record
+// layout 30-48, access 199-228, collision 612-699, level kernels 702-793) and
+// crates/cfd/src/d3q27.rs.
+//
+// HBM layout of a level: two population sets (A/B) of 27 planes each, set s
+// direction i of cell n at (s * 27 + i) * NP + n, the plane stride NP being
+// the cell count rounded up to 256 (every plane 512-byte aligned at 2-byte
+// storage).  One u32 flag per cell: type in the low 3 bits (0 fluid, 1 solid,
+// 2 face, 3 ghost, 4 restricted), wall record + 1 (or the face kind) above.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "lbm_device.cuh"
+
+namespace lbm27 {
+
+constexpr uint32_t RS = 24, R_MASK = 0, R_CELL = 1, R_Q = 2, R_FT = 15;  // record words (mshader.rs:32-36)
+constexpr uint32_t MW = 12;                                               // words per exported moment node
+constexpr uint32_t T_FLUID = 0, T_SOLID = 1, T_FACE = 2, T_GHOST = 3, T_RESTRICT = 4;
+
+template <class R>
+struct Consts27 {
+    R tau0, smag2, sponge_tau, sigma;
+    R sp_lo[3], sp_hi[3], u_inf[3], u_init[3], grav[3], center[3];
+};
+
+struct LevelParams {
+    void *pop;                  // 2 sets x 27 planes of NP cells
+    uint64_t NP;
+    uint32_t *flags;
+    const uint32_t *faces, *ghosts, *restricted;
+    uint32_t nface, nghost, nrestrict;
+    uint32_t NX, NY, NZ, N;
+    lbm::FastDiv div_nx, div_nxy;
+    int per[3];
+    int n_sponge, forcing, abs_u, total_p;
+    // refinement: this level's exports and the neighbouring levels' buffers
+    int has_child, has_parent;
+    int ch_lo[3];
+    uint32_t ch_n[3];           // the child box in this level's nodes
+    uint32_t ch_nodes;
+    uint32_t pn[3];             // this level's nodes seen from its parent ((d - 1) / 2 + 1)
+    void *mom_child;            // R, 2 slots x ch_nodes x MW: surface moments for the child's ghosts
+    void *mom_up;               // R, pn nodes x MW: even-node moments for the parent's restriction
+    const void *mom_parent;     // the parent's mom_child (ghost fill)
+    const void *mom_child_up;   // the child's mom_up (restriction)
+    // wall records (finest level only; nrec = 0 elsewhere)
+    uint32_t *recs;
+    double *recd;               // FP64 engine: 6 doubles (F, T) per record
+    uint32_t nrec;
+    float4 *dump;
+    Consts27<float> kf;
+    Consts27<double> kd;
+};
+
+struct StepArgs {
+    uint32_t src;       // source population set
+    uint32_t mw;        // moment slot this step writes (mom_child)
+    uint32_t mold, mnew;  // ghost fill: the parent's moment slots at the start and end of its step
+    uint32_t seed_mix;  // stochastic rounding: the step seed's term of the hash
+    float blend;        // ghost fill: time fraction between mold and mnew
+    float omega[3];     // wall angular velocity, rad per finest step
+    double omega_d[3];
+};
+
+// storage: lbm_storage (0 FP32, 1 FP16, 2 BF16, 3 FP64)
+cudaError_t launch27_init(int storage, const LevelParams &p, cudaStream_t st);
+cudaError_t launch27_face(int storage, const LevelParams &p, const StepArgs &a, cudaStream_t st);
+cudaError_t launch27_step(int storage, const LevelParams &p, const StepArgs &a, cudaStream_t st);
+cudaError_t launch27_ghost(int storage, const LevelParams &p, const StepArgs &a, cudaStream_t st);
+cudaError_t launch27_restrict(int storage, const LevelParams &p, const StepArgs &a, cudaStream_t st);
+cudaError_t launch27_dump(int storage, const LevelParams &p, uint32_t src, cudaStream_t st);
+cudaError_t launch27_mass(int storage, const LevelParams &p, uint32_t src, double *mass, unsigned long long *bad, cudaStream_t st);
+// FP64 sum of the records' force and moment into out[0..5] (deterministic
+// order: per-block partials, the last block sums them)
+cudaError_t launch27_reduce(const LevelParams &p, int fp64, double *partials, uint32_t *ticket, double *out, cudaStream_t st);
+uint32_t reduce27_blocks(uint32_t nrec);
+
+}  // namespace lbm27

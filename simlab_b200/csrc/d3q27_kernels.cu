@@ -1,0 +1,736 @@
+// Multi-level D3Q27 kernels for sm_100a.
+//
+// One level step (crates/cfd/src/mshader.rs:612-699): each fluid cell pulls
+// the post-collision populations of its 26 neighbours from the source set,
+// applies Bouzidi bounce-back with moving-wall momentum exchange on its cut
+// links (mshader.rs:364-403), takes moments, relaxes the deviatoric second
+// central moments with the viscous rate (Smagorinsky and sponge on tau), sets
+// the trace and every higher cumulant to equilibrium, rebuilds the
+// populations of that Gaussian by backward central-moment transforms (`gauss`,
+// mshader.rs:286-362), adds the absorbing layer and writes the result to the
+// destination set.  Cells on a child box surface export their moments for the
+// child's ghosts; even nodes of a refined level export theirs for the
+// parent's restriction.
+//
+// Level kernels (mshader.rs:702-793): domain faces rebuilt from the interior
+// cell, fine ghosts interpolated in space and time from the parent's surface
+// moments with the Dupuis-Chopard stress rescale, coarse cells under the child
+// box restricted from the coincident fine nodes.
+//
+// Memory-bound (220 B per cell update in FP32, 112 B in FP16/BF16): one thread
+// per cell, 27 coalesced loads from the source planes (x-shifted loads served
+// by L1), 27 coalesced stores.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <type_traits>
+
+#include "d3q27.h"
+
+namespace lbm27 {
+
+using lbm::FastDiv;
+using lbm::Pop;
+using lbm::Rng;
+
+constexpr int BLK = 256;
+
+__host__ __device__ __forceinline__ constexpr int CX(int i) { return i % 3 - 1; }
+__host__ __device__ __forceinline__ constexpr int CY(int i) { return (i / 3) % 3 - 1; }
+__host__ __device__ __forceinline__ constexpr int CZ(int i) { return i / 9 - 1; }
+__host__ __device__ __forceinline__ constexpr int SLOT(int i) { return i < 13 ? i : i - 1; }
+__host__ __device__ __forceinline__ constexpr double WD(int i) {
+    return (CX(i) * CX(i) + CY(i) * CY(i) + CZ(i) * CZ(i)) == 0 ? 8.0 / 27.0
+         : (CX(i) * CX(i) + CY(i) * CY(i) + CZ(i) * CZ(i)) == 1 ? 2.0 / 27.0
+         : (CX(i) * CX(i) + CY(i) * CY(i) + CZ(i) * CZ(i)) == 2 ? 1.0 / 54.0
+                                                                 : 1.0 / 216.0;
+}
+template <class R> __device__ __forceinline__ R W(int i) { return (R)WD(i); }
+template <> __device__ __forceinline__ float W<float>(int i) { return (float)WD(i); }
+template <class R> __device__ __forceinline__ R W45(int i) { return (R)(4.5 * WD(i)); }
+
+template <class R> __device__ __forceinline__ const Consts27<R> &K(const LevelParams &p);
+template <> __device__ __forceinline__ const Consts27<float> &K<float>(const LevelParams &p) { return p.kf; }
+template <> __device__ __forceinline__ const Consts27<double> &K<double>(const LevelParams &p) { return p.kd; }
+
+__device__ __forceinline__ void coords(const LevelParams &p, uint32_t n, uint32_t &x, uint32_t &y, uint32_t &z) {
+    z = p.div_nxy.div(n);
+    const uint32_t r = n - z * (p.NX * p.NY);
+    y = p.div_nx.div(r);
+    x = r - y * p.NX;
+}
+
+template <class S>
+__device__ __forceinline__ const S *set_ptr(const LevelParams &p, uint32_t set) { return (const S *)p.pop + (uint64_t)set * 27u * p.NP; }
+template <class S>
+__device__ __forceinline__ S *set_ptr_w(const LevelParams &p, uint32_t set) { return (S *)p.pop + (uint64_t)set * 27u * p.NP; }
+
+// own post-collision populations of cell n (mshader.rs:201-206)
+template <class S>
+__device__ __forceinline__ void own(const LevelParams &p, uint32_t set, uint32_t n, typename Pop<S>::real *f) {
+    const S *s = set_ptr<S>(p, set);
+#pragma unroll
+    for (int i = 0; i < 27; i++) f[i] = Pop<S>::ld(s + (uint64_t)i * p.NP + n);
+}
+// writes a full post-collision state (mshader.rs:207-217)
+template <class S>
+__device__ __forceinline__ void put(const LevelParams &p, uint32_t set, uint32_t n, const typename Pop<S>::real *f, Rng &rng) {
+    S *s = set_ptr_w<S>(p, set);
+#pragma unroll
+    for (int i = 0; i < 27; i++) s[(uint64_t)i * p.NP + n] = Pop<S>::enc(f[i], rng);
+}
+
+template <class R>
+struct Mom {
+    R rho1, j[3], s[6];
+};
+
+// mshader.rs:236-255
+template <class R>
+__device__ __forceinline__ Mom<R> moments(const R *f) {
+    // sums over the x-rows (cy, cz fixed): row totals and x-differences
+    R rs[9], rd[9];
+#pragma unroll
+    for (int r = 0; r < 9; r++) {
+        rs[r] = (f[3 * r] + f[3 * r + 1]) + f[3 * r + 2];
+        rd[r] = f[3 * r + 2] - f[3 * r];
+    }
+    Mom<R> m;
+    // rows r = (cy + 1) + 3 (cz + 1)
+    const R zm = (rs[0] + rs[1]) + rs[2], z0 = (rs[3] + rs[4]) + rs[5], zp = (rs[6] + rs[7]) + rs[8];
+    m.rho1 = (zm + z0) + zp;
+    m.j[0] = ((rd[0] + rd[1]) + rd[2]) + ((rd[3] + rd[4]) + rd[5]) + ((rd[6] + rd[7]) + rd[8]);
+    const R ym = (rs[0] + rs[3]) + rs[6], yp = (rs[2] + rs[5]) + rs[8];
+    m.j[1] = yp - ym;
+    m.j[2] = zp - zm;
+    // sxx: rows' f[+x] + f[-x]
+    R sx = 0;
+#pragma unroll
+    for (int r = 0; r < 9; r++) sx += f[3 * r] + f[3 * r + 2];
+    m.s[0] = sx;
+    m.s[1] = ym + yp;
+    m.s[2] = zm + zp;
+    // sxy = sum cx cy f: rows with cy = +1 minus rows with cy = -1 of rd
+    m.s[3] = ((rd[2] + rd[5]) + rd[8]) - ((rd[0] + rd[3]) + rd[6]);
+    m.s[4] = ((rd[6] + rd[7]) + rd[8]) - ((rd[0] + rd[1]) + rd[2]);
+    m.s[5] = (rs[8] - rs[6]) - (rs[2] - rs[0]);
+    return m;
+}
+
+// mshader.rs:257-266: product-form equilibrium, shifted
+template <class R>
+__device__ __forceinline__ void feq(R rho, R ux, R uy, R uz, R *f) {
+    const R third = (R)1 / (R)3, two3 = (R)2 / (R)3, h = (R)0.5;
+    const R u[3] = {ux, uy, uz};
+    R a[3][3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const R uu = u[k] * u[k];
+        a[k][0] = h * (third + uu - u[k]);
+        a[k][1] = two3 - uu;
+        a[k][2] = h * (third + uu + u[k]);
+    }
+#pragma unroll
+    for (int i = 0; i < 27; i++) f[i] = rho * a[0][CX(i) + 1] * a[1][CY(i) + 1] * a[2][CZ(i) + 1] - W<R>(i);
+}
+
+// mshader.rs:268-280: 4.5 w (c c : p - tr p / 3)
+template <class R>
+__device__ __forceinline__ void fneq_add(const R *p, R *f) {
+    const R tr = (p[0] + p[1] + p[2]) * ((R)1 / (R)3);
+#pragma unroll
+    for (int i = 0; i < 27; i++) {
+        R t = -tr;
+        if (CX(i) != 0) t = t + p[0];
+        if (CY(i) != 0) t = t + p[1];
+        if (CZ(i) != 0) t = t + p[2];
+        if (CX(i) * CY(i) != 0) t = t + (R)(2 * CX(i) * CY(i)) * p[3];
+        if (CX(i) * CZ(i) != 0) t = t + (R)(2 * CX(i) * CZ(i)) * p[4];
+        if (CY(i) * CZ(i) != 0) t = t + (R)(2 * CY(i) * CZ(i)) * p[5];
+        f[i] += W45<R>(i) * t;
+    }
+}
+
+// mshader.rs:486-501
+template <class R>
+__device__ __forceinline__ void stress(const Mom<R> &mo, R rho, const R *u, R *p) {
+    const R r3 = mo.rho1 / (R)3;
+    p[0] = mo.s[0] - rho * u[0] * u[0] - r3;
+    p[1] = mo.s[1] - rho * u[1] * u[1] - r3;
+    p[2] = mo.s[2] - rho * u[2] * u[2] - r3;
+    p[3] = mo.s[3] - rho * u[0] * u[1];
+    p[4] = mo.s[4] - rho * u[0] * u[2];
+    p[5] = mo.s[5] - rho * u[1] * u[2];
+}
+template <class R>
+__device__ __forceinline__ void deviator(const R *p, R *d) {
+    const R tr = (p[0] + p[1] + p[2]) / (R)3;
+    d[0] = p[0] - tr; d[1] = p[1] - tr; d[2] = p[2] - tr;
+    d[3] = p[3]; d[4] = p[4]; d[5] = p[5];
+}
+// mshader.rs:503-509: a post-collision state from rho, u and a stress
+template <class R>
+__device__ __forceinline__ void rebuild(R rho, const R *u, const R *pp, R *f) {
+    feq<R>(rho, u[0], u[1], u[2], f);
+    R d[6];
+    deviator<R>(pp, d);
+    fneq_add<R>(d, f);
+}
+
+// one backward central-moment transform along an axis (mshader.rs:316-322):
+// central moments (k0, k1, k2) about velocity w -> populations (-1, 0, +1)
+template <class R>
+__device__ __forceinline__ void back(R k0, R k1, R k2, R w, R &m, R &o, R &pl) {
+    const R r1 = k1 + w * k0;
+    const R r2 = k2 + (R)2 * w * k1 + w * w * k0;
+    m = (R)0.5 * (r2 - r1);
+    o = k0 - r2;
+    pl = (R)0.5 * (r2 + r1);
+}
+// the same with k1 = 0 (the odd central moments that vanish without forcing)
+template <class R>
+__device__ __forceinline__ void back0(R k0, R k2, R w, R &m, R &o, R &pl) {
+    const R r1 = w * k0;
+    const R r2 = k2 + w * w * k0;
+    m = (R)0.5 * (r2 - r1);
+    o = k0 - r2;
+    pl = (R)0.5 * (r2 + r1);
+}
+// the same with k0 = k2 = 0
+template <class R>
+__device__ __forceinline__ void back_odd(R k1, R w, R &m, R &o, R &pl) {
+    const R r1 = k1;
+    const R r2 = (R)2 * w * k1;
+    m = (R)0.5 * (r2 - r1);
+    o = -r2;
+    pl = (R)0.5 * (r2 + r1);
+}
+
+// mshader.rs:286-362: populations (shifted) of the Gaussian with covariance
+// sg (xx yy zz xy xz yz) and first central moments m1, higher cumulants zero
+template <class R, bool FORCE>
+__device__ __forceinline__ void gauss(R rho, const R *u, const R *sg, const R *m1, R *f) {
+    const R a = sg[0], b = sg[1], cc = sg[2], d = sg[3], e = sg[4], g = sg[5];
+    const R two = 2;
+    // z pass: Z[i][j][cz] from k_ij0, k_ij1, k_ij2
+    R Z[3][3][3];
+    const R k000 = rho, k200 = rho * a, k020 = rho * b, k002 = rho * cc, k110 = rho * d, k101 = rho * e, k011 = rho * g;
+    const R k220 = rho * (a * b + two * d * d), k202 = rho * (a * cc + two * e * e), k022 = rho * (b * cc + two * g * g);
+    const R k211 = rho * (a * g + two * d * e), k121 = rho * (b * e + two * d * g), k112 = rho * (cc * d + two * e * g);
+    const R k222 = rho * (a * b * cc + two * (a * g * g + b * e * e + cc * d * d) + (R)8 * d * e * g);
+    const R w = u[2];
+    if (FORCE) {
+        const R k100 = rho * m1[0], k010 = rho * m1[1], k001 = rho * m1[2];
+        back<R>(k000, k001, k002, w, Z[0][0][0], Z[0][0][1], Z[0][0][2]);
+        back<R>(k100, k101, (R)0, w, Z[1][0][0], Z[1][0][1], Z[1][0][2]);
+        back<R>(k010, k011, (R)0, w, Z[0][1][0], Z[0][1][1], Z[0][1][2]);
+    } else {
+        back0<R>(k000, k002, w, Z[0][0][0], Z[0][0][1], Z[0][0][2]);
+        back_odd<R>(k101, w, Z[1][0][0], Z[1][0][1], Z[1][0][2]);
+        back_odd<R>(k011, w, Z[0][1][0], Z[0][1][1], Z[0][1][2]);
+    }
+    back0<R>(k200, k202, w, Z[2][0][0], Z[2][0][1], Z[2][0][2]);
+    back0<R>(k110, k112, w, Z[1][1][0], Z[1][1][1], Z[1][1][2]);
+    back_odd<R>(k211, w, Z[2][1][0], Z[2][1][1], Z[2][1][2]);
+    back0<R>(k020, k022, w, Z[0][2][0], Z[0][2][1], Z[0][2][2]);
+    back_odd<R>(k121, w, Z[1][2][0], Z[1][2][1], Z[1][2][2]);
+    back0<R>(k220, k222, w, Z[2][2][0], Z[2][2][1], Z[2][2][2]);
+    // y pass: Y[i][cz][cy]
+    R Y[3][3][3];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) back<R>(Z[i][0][c], Z[i][1][c], Z[i][2][c], u[1], Y[i][c][0], Y[i][c][1], Y[i][c][2]);
+    // x pass: f(cx, cy, cz)
+#pragma unroll
+    for (int cyi = 0; cyi < 3; cyi++)
+#pragma unroll
+        for (int czi = 0; czi < 3; czi++) {
+            R m, o, pl;
+            back<R>(Y[0][czi][cyi], Y[1][czi][cyi], Y[2][czi][cyi], u[0], m, o, pl);
+            const int base = 3 * cyi + 9 * czi;  // direction of (cx = -1, cy, cz)
+            f[base] = m - W<R>(base);
+            f[base + 1] = o - W<R>(base + 1);
+            f[base + 2] = pl - W<R>(base + 2);
+        }
+}
+
+template <class R>
+__device__ __forceinline__ R sponge(const LevelParams &p, const Consts27<R> &k, uint32_t x, uint32_t y, uint32_t z) {
+    const R pp[3] = {(R)(float)x, (R)(float)y, (R)(float)z};
+    const R hi[3] = {(R)(float)(p.NX - 1) - pp[0], (R)(float)(p.NY - 1) - pp[1], (R)(float)(p.NZ - 1) - pp[2]};
+    R s = 0;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        if (k.sp_lo[a] > (R)0) s = max(s, (R)1 - pp[a] / k.sp_lo[a]);
+        if (k.sp_hi[a] > (R)0) s = max(s, (R)1 - hi[a] / k.sp_hi[a]);
+    }
+    return min(max(s, (R)0), (R)1);
+}
+
+template <class S>
+__device__ __forceinline__ Rng cell_rng(uint32_t n, uint32_t seed_mix) {
+    Rng r;
+    r.s = lbm::sr_hash_mix(n, seed_mix);
+    return r;
+}
+
+// ------------------------------------------------------------ the step
+template <class S, bool FORCE>
+__global__ void __launch_bounds__(BLK) k27_step(const __grid_constant__ LevelParams p, const StepArgs a) {
+    using R = typename Pop<S>::real;
+    const uint32_t n = blockIdx.x * BLK + threadIdx.x;
+    if (n >= p.N) return;
+    const uint32_t fg = p.flags[n];
+    if ((fg & 7u) != 0) return;
+    const Consts27<R> &k = K<R>(p);
+    uint32_t x, y, z;
+    coords(p, n, x, y, z);
+    // neighbour rows with periodic wrap (mshader.rs:135-138)
+    const uint32_t xi[3] = {x == 0 ? p.NX - 1 : x - 1, x, x == p.NX - 1 ? 0 : x + 1};
+    const uint32_t yi[3] = {y == 0 ? p.NY - 1 : y - 1, y, y == p.NY - 1 ? 0 : y + 1};
+    const uint32_t zi[3] = {z == 0 ? p.NZ - 1 : z - 1, z, z == p.NZ - 1 ? 0 : z + 1};
+    const S *src = set_ptr<S>(p, a.src);
+    R f[27];
+    // pull: the population moving along c_i comes from n - c_i
+#pragma unroll
+    for (int i = 0; i < 27; i++) {
+        const uint32_t m = (zi[1 - CZ(i)] * p.NY + yi[1 - CY(i)]) * p.NX + xi[1 - CX(i)];
+        f[i] = Pop<S>::ld(src + (uint64_t)i * p.NP + m);
+    }
+    const uint32_t rec = fg >> 3;
+    R Fv[3] = {0, 0, 0}, Tv[3] = {0, 0, 0};
+    if (rec != 0) {
+        const uint32_t r = rec - 1;
+        const uint32_t mask = p.recs[r * RS + R_MASK];
+        R fin[27];
+#pragma unroll
+        for (int i = 0; i < 27; i++) fin[i] = f[i];
+        const R pc[3] = {(R)(float)x - k.center[0], (R)(float)y - k.center[1], (R)(float)z - k.center[2]};
+        R om[3];
+        if (sizeof(R) == 8) { om[0] = (R)a.omega_d[0]; om[1] = (R)a.omega_d[1]; om[2] = (R)a.omega_d[2]; }
+        else { om[0] = (R)a.omega[0]; om[1] = (R)a.omega[1]; om[2] = (R)a.omega[2]; }
+#pragma unroll
+        for (int i = 0; i < 27; i++) {
+            if (i == 13) continue;
+            if (!(mask & (1u << i))) continue;
+            const int o = 26 - i;
+            const uint32_t wq = p.recs[r * RS + R_Q + SLOT(i) / 2];
+            const uint16_t hq = (SLOT(i) & 1) ? (uint16_t)(wq >> 16) : (uint16_t)(wq & 0xffffu);
+            const R q = max((R)__half2float(__ushort_as_half(hq)), (R)0.001f);
+            const R fpi = Pop<S>::ld(src + (uint64_t)i * p.NP + n) + W<R>(i);
+            const R fpo = Pop<S>::ld(src + (uint64_t)o * p.NP + n) + W<R>(i);
+            const R ci[3] = {(R)CX(i), (R)CY(i), (R)CZ(i)};
+            const R xw[3] = {pc[0] + q * ci[0], pc[1] + q * ci[1], pc[2] + q * ci[2]};
+            const R uw[3] = {om[1] * xw[2] - om[2] * xw[1], om[2] * xw[0] - om[0] * xw[2], om[0] * xw[1] - om[1] * xw[0]};
+            const R cu = ci[0] * uw[0] + ci[1] * uw[1] + ci[2] * uw[2];
+            const R w6 = (R)6 * W<R>(i);
+            R fb;
+            if (q >= (R)0.5) fb = (fpi + ((R)2 * q - (R)1) * fpo - w6 * cu) / ((R)2 * q);
+            else if (!(mask & (1u << o))) fb = (R)2 * q * fpi + ((R)1 - (R)2 * q) * (fin[i] + W<R>(i)) - w6 * cu;
+            else fb = fpi - w6 * cu;
+            f[o] = fb - W<R>(i);
+            R flk[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) flk[c] = (ci[c] - uw[c]) * fpi + (ci[c] + uw[c]) * fb;
+#pragma unroll
+            for (int c = 0; c < 3; c++) Fv[c] += flk[c];
+            Tv[0] += xw[1] * flk[2] - xw[2] * flk[1];
+            Tv[1] += xw[2] * flk[0] - xw[0] * flk[2];
+            Tv[2] += xw[0] * flk[1] - xw[1] * flk[0];
+        }
+    }
+    const Mom<R> mo = moments<R>(f);
+    const R rho = (R)1 + mo.rho1;
+    const R inv_rho = (R)1 / rho;
+    R G[3] = {0, 0, 0}, u[3];
+    if (FORCE) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) G[c] = rho * k.grav[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) u[c] = FORCE ? (mo.j[c] + (R)0.5 * G[c]) * inv_rho : mo.j[c] * inv_rho;
+    R pst[6];
+    stress<R>(mo, rho, u, pst);
+    R dv[6];
+    deviator<R>(pst, dv);
+    R tau = k.tau0;
+    if (k.smag2 > (R)0) {
+        const R pp = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2] + (R)2 * (dv[3] * dv[3] + dv[4] * dv[4] + dv[5] * dv[5]);
+        tau = (R)0.5 * (k.tau0 + sqrt(k.tau0 * k.tau0 + (R)18 * k.smag2 * sqrt((R)2 * pp) * inv_rho));
+    }
+    R sp = 0;
+    if (p.n_sponge) {
+        sp = sponge<R>(p, k, x, y, z);
+        if (sp > (R)0 && k.sponge_tau > tau) tau += sp * sp * (k.sponge_tau - tau);
+    }
+    const R om1 = (R)1 - (R)1 / tau;
+    const R third = (R)1 / (R)3;
+    R sg[6];
+#pragma unroll
+    for (int c = 0; c < 3; c++) sg[c] = third + om1 * dv[c] * inv_rho;
+#pragma unroll
+    for (int c = 3; c < 6; c++) sg[c] = om1 * dv[c] * inv_rho;
+    R m1[3] = {0, 0, 0};
+    if (FORCE) {
+#pragma unroll
+        for (int c = 0; c < 3; c++) m1[c] = (R)0.5 * G[c] * inv_rho;
+    }
+    R fo[27];
+    gauss<R, FORCE>(rho, u, sg, m1, fo);
+    if (p.n_sponge && k.sigma > (R)0 && sp > (R)0) {
+        // absorbing layer: pull density (and with abs_u, velocity) toward the far field
+        R ft[27], fc[27];
+        if (p.abs_u) feq<R>((R)1, k.u_inf[0], k.u_inf[1], k.u_inf[2], ft);
+        else feq<R>((R)1, u[0], u[1], u[2], ft);
+        feq<R>(rho, u[0], u[1], u[2], fc);
+        const R sgm = k.sigma * sp * sp;
+#pragma unroll
+        for (int i = 0; i < 27; i++) fo[i] += sgm * (ft[i] - fc[i]);
+    }
+    if (rec != 0) {
+        const uint32_t r = rec - 1;
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            p.recs[r * RS + R_FT + c] = __float_as_uint((float)Fv[c]);
+            p.recs[r * RS + R_FT + 3 + c] = __float_as_uint((float)Tv[c]);
+        }
+        if (p.recd) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) { p.recd[r * 6 + c] = (double)Fv[c]; p.recd[r * 6 + 3 + c] = (double)Tv[c]; }
+        }
+    }
+    Rng rng = cell_rng<S>(n, a.seed_mix);
+    put<S>(p, 1u - a.src, n, fo, rng);
+    // moments for the finer level's ghosts (child box surface)
+    if (p.has_child) {
+        const int lx = (int)x - p.ch_lo[0], ly = (int)y - p.ch_lo[1], lz = (int)z - p.ch_lo[2];
+        if (lx >= 0 && ly >= 0 && lz >= 0 && lx < (int)p.ch_n[0] && ly < (int)p.ch_n[1] && lz < (int)p.ch_n[2] &&
+            (lx == 0 || ly == 0 || lz == 0 || lx == (int)p.ch_n[0] - 1 || ly == (int)p.ch_n[1] - 1 || lz == (int)p.ch_n[2] - 1)) {
+            R *o = (R *)p.mom_child + ((uint64_t)a.mw * p.ch_nodes + ((uint64_t)lz * p.ch_n[1] + ly) * p.ch_n[0] + lx) * MW;
+            o[0] = rho; o[1] = u[0]; o[2] = u[1]; o[3] = u[2];
+#pragma unroll
+            for (int c = 0; c < 6; c++) o[4 + c] = pst[c];
+            o[10] = tau;
+        }
+    }
+    // moments for the coarser level's restriction (the nodes it shares)
+    if (p.has_parent && ((x | y | z) & 1u) == 0) {
+        R *o = (R *)p.mom_up + (((uint64_t)(z >> 1) * p.pn[1] + (y >> 1)) * p.pn[0] + (x >> 1)) * MW;
+        o[0] = rho; o[1] = u[0]; o[2] = u[1]; o[3] = u[2];
+#pragma unroll
+        for (int c = 0; c < 6; c++) o[4 + c] = pst[c];
+        o[10] = tau;
+    }
+}
+
+// ------------------------------------------------------------ level kernels
+// mshader.rs:702-733: domain faces of the coarsest level
+template <class S>
+__global__ void __launch_bounds__(BLK) k27_face(const __grid_constant__ LevelParams p, const StepArgs a) {
+    using R = typename Pop<S>::real;
+    const uint32_t kk = blockIdx.x * BLK + threadIdx.x;
+    if (kk >= p.nface) return;
+    const Consts27<R> &k = K<R>(p);
+    const uint32_t b = p.faces[kk];
+    uint32_t x, y, z;
+    coords(p, b, x, y, z);
+    if (!p.per[0]) x = min(max(x, 1u), p.NX - 2);
+    if (!p.per[1]) y = min(max(y, 1u), p.NY - 2);
+    if (!p.per[2]) z = min(max(z, 1u), p.NZ - 2);
+    const uint32_t m = (z * p.NY + y) * p.NX + x;
+    R rho = 1, u[3] = {k.u_inf[0], k.u_inf[1], k.u_inf[2]}, pp[6] = {0, 0, 0, 0, 0, 0};
+    if ((p.flags[m] & 7u) == 0) {
+        R f[27];
+        own<S>(p, a.src, m, f);
+        const Mom<R> mo = moments<R>(f);
+        rho = (R)1 + mo.rho1;
+#pragma unroll
+        for (int c = 0; c < 3; c++) u[c] = mo.j[c] / rho;
+        stress<R>(mo, rho, u, pp);
+    }
+    const uint32_t ty = (p.flags[b] >> 3) & 3u;
+    if (ty == 1) {
+        if (p.total_p) {
+            const R third = (R)1 / (R)3;
+            const R ui2 = k.u_inf[0] * k.u_inf[0] + k.u_inf[1] * k.u_inf[1] + k.u_inf[2] * k.u_inf[2];
+            const R u2 = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+            rho = (third + (R)0.5 * ui2) / (third + (R)0.5 * u2);
+        } else {
+            u[0] = k.u_inf[0]; u[1] = k.u_inf[1]; u[2] = k.u_inf[2];
+        }
+    } else {
+        rho = 1;
+    }
+    R f[27];
+    rebuild<R>(rho, u, pp, f);
+    Rng rng = cell_rng<S>(b, a.seed_mix);
+    put<S>(p, a.src, b, f, rng);
+}
+
+// mshader.rs:742-775: fine ghosts from the parent's surface moments, linear in
+// space and time, stress rescaled for half the time step
+template <class S>
+__global__ void __launch_bounds__(BLK) k27_ghost(const __grid_constant__ LevelParams p, const StepArgs a) {
+    using R = typename Pop<S>::real;
+    const uint32_t kk = blockIdx.x * BLK + threadIdx.x;
+    if (kk >= p.nghost) return;
+    const uint32_t n = p.ghosts[kk];
+    uint32_t xyz[3];
+    coords(p, n, xyz[0], xyz[1], xyz[2]);
+    const uint32_t h0[3] = {xyz[0] >> 1, xyz[1] >> 1, xyz[2] >> 1};
+    const uint32_t odd[3] = {xyz[0] & 1u, xyz[1] & 1u, xyz[2] & 1u};
+    const R *mp = (const R *)p.mom_parent;
+    const uint64_t pnodes = (uint64_t)p.pn[0] * p.pn[1] * p.pn[2];
+    R acc[11];
+#pragma unroll
+    for (int j = 0; j < 11; j++) acc[j] = 0;
+    R wsum = 0;
+    const R blend = (R)a.blend;
+#pragma unroll
+    for (uint32_t c = 0; c < 8; c++) {
+        const uint32_t o[3] = {c & 1u, (c >> 1) & 1u, (c >> 2) & 1u};
+        if ((o[0] & ~odd[0]) | (o[1] & ~odd[1]) | (o[2] & ~odd[2])) continue;
+        const R w = (odd[0] ? (R)0.5 : (R)1) * (odd[1] ? (R)0.5 : (R)1) * (odd[2] ? (R)0.5 : (R)1);
+        const uint64_t nd = ((uint64_t)(h0[2] + o[2]) * p.pn[1] + (h0[1] + o[1])) * p.pn[0] + (h0[0] + o[0]);
+        const R *ma = mp + (a.mold * pnodes + nd) * MW;
+        const R *mb = mp + (a.mnew * pnodes + nd) * MW;
+#pragma unroll
+        for (int j = 0; j < 11; j++) acc[j] += w * (((R)1 - blend) * ma[j] + blend * mb[j]);
+        wsum += w;
+    }
+    const R rho = acc[0] / wsum;
+    const R u[3] = {acc[1] / wsum, acc[2] / wsum, acc[3] / wsum};
+    const R tc = acc[10] / wsum;
+    const R tf = (R)0.5 + (R)2 * (tc - (R)0.5);
+    const R sc = tf / ((R)2 * tc) * ((R)1 - (R)1 / tf);
+    R pp[6];
+#pragma unroll
+    for (int j = 0; j < 6; j++) pp[j] = acc[4 + j] / wsum * sc;
+    R f[27];
+    rebuild<R>(rho, u, pp, f);
+    Rng rng = cell_rng<S>(n, a.seed_mix);
+    put<S>(p, a.src, n, f, rng);
+}
+
+// mshader.rs:777-793: coarse cells under the child box from its coincident nodes
+template <class S>
+__global__ void __launch_bounds__(BLK) k27_restrict(const __grid_constant__ LevelParams p, const StepArgs a) {
+    using R = typename Pop<S>::real;
+    const uint32_t kk = blockIdx.x * BLK + threadIdx.x;
+    if (kk >= p.nrestrict) return;
+    const uint32_t n = p.restricted[kk];
+    uint32_t x, y, z;
+    coords(p, n, x, y, z);
+    const uint32_t lx = x - (uint32_t)p.ch_lo[0], ly = y - (uint32_t)p.ch_lo[1], lz = z - (uint32_t)p.ch_lo[2];
+    const R *m = (const R *)p.mom_child_up + (((uint64_t)lz * p.ch_n[1] + ly) * p.ch_n[0] + lx) * MW;
+    const R rho = m[0];
+    const R u[3] = {m[1], m[2], m[3]};
+    const R tf = m[10];
+    const R tc = (R)0.5 + (R)0.5 * (tf - (R)0.5);
+    const R sc = (R)2 * tc / tf * ((R)1 - (R)1 / tc);
+    R pp[6];
+#pragma unroll
+    for (int j = 0; j < 6; j++) pp[j] = m[4 + j] * sc;
+    R f[27];
+    rebuild<R>(rho, u, pp, f);
+    Rng rng = cell_rng<S>(n, a.seed_mix);
+    put<S>(p, a.src, n, f, rng);
+}
+
+// mshader.rs:520-527: feq(1, u_init) in both sets
+template <class S>
+__global__ void __launch_bounds__(BLK) k27_init(const __grid_constant__ LevelParams p) {
+    using R = typename Pop<S>::real;
+    const uint32_t n = blockIdx.x * BLK + threadIdx.x;
+    if (n >= p.N) return;
+    const Consts27<R> &k = K<R>(p);
+    R f[27];
+    feq<R>((R)1, k.u_init[0], k.u_init[1], k.u_init[2], f);
+    Rng rng = cell_rng<S>(n, 0x632BE5ABu);
+    put<S>(p, 0, n, f, rng);
+    rng = cell_rng<S>(n, 0x632BE5ABu);
+    put<S>(p, 1, n, f, rng);
+}
+
+// mshader.rs:495-505, 602-610
+template <class S>
+__global__ void __launch_bounds__(BLK) k27_dump(const __grid_constant__ LevelParams p, uint32_t src) {
+    using R = typename Pop<S>::real;
+    const uint32_t n = blockIdx.x * BLK + threadIdx.x;
+    if (n >= p.N) return;
+    const Consts27<R> &k = K<R>(p);
+    if ((p.flags[n] & 7u) != 0) {
+        const float nan = __int_as_float(0x7fc00000);
+        p.dump[n] = make_float4(nan, nan, nan, nan);
+        return;
+    }
+    R f[27];
+    own<S>(p, src, n, f);
+    const Mom<R> mo = moments<R>(f);
+    const R rho = (R)1 + mo.rho1;
+    p.dump[n] = make_float4((float)rho, (float)(mo.j[0] / rho - (R)0.5 * k.grav[0]), (float)(mo.j[1] / rho - (R)0.5 * k.grav[1]),
+                            (float)(mo.j[2] / rho - (R)0.5 * k.grav[2]));
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <class S>
+__global__ void __launch_bounds__(BLK) k27_mass(const __grid_constant__ LevelParams p, uint32_t src, double *mass, unsigned long long *bad) {
+    using R = typename Pop<S>::real;
+    const uint32_t n = blockIdx.x * BLK + threadIdx.x;
+    double m = 0;
+    unsigned nb = 0;
+    if (n < p.N && (p.flags[n] & 7u) == 0) {
+        R f[27];
+        own<S>(p, src, n, f);
+        double s = 1.0;
+#pragma unroll
+        for (int i = 0; i < 27; i++) s += (double)f[i];
+        if (isfinite(s)) m = s;
+        else nb = 1;
+    }
+    m = warp_sum(m);
+    nb = __reduce_add_sync(0xffffffffu, nb);
+    if ((threadIdx.x & 31) == 0) {
+        if (m != 0.0) atomicAdd(mass, m);
+        if (nb) atomicAdd(bad, (unsigned long long)nb);
+    }
+}
+
+// FP64 sum of the records' force and moment: per-block partials in fixed
+// order, the last block to finish sums the partials (mshader.rs:519-562 does
+// the same sum in f32)
+constexpr uint32_t RED_BLK = 256;
+template <bool FP64>
+__global__ void __launch_bounds__(RED_BLK) k27_reduce(const __grid_constant__ LevelParams p, double *partials, uint32_t *ticket, double *out) {
+    const uint32_t r = blockIdx.x * RED_BLK + threadIdx.x;
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    if (r < p.nrec) {
+#pragma unroll
+        for (int j = 0; j < 6; j++) v[j] = FP64 ? p.recd[(uint64_t)r * 6 + j] : (double)__uint_as_float(p.recs[(uint64_t)r * RS + R_FT + j]);
+    }
+    __shared__ double sh[RED_BLK / 32][6];
+    __shared__ bool last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < 6; j++) v[j] = warp_sum(v[j]);
+    if (lane == 0)
+        for (int j = 0; j < 6; j++) sh[warp][j] = v[j];
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double t = 0;
+        for (int w = 0; w < (int)(RED_BLK / 32); w++) t += sh[w][threadIdx.x];
+        partials[blockIdx.x * 8 + threadIdx.x] = t;
+        __threadfence();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += RED_BLK)
+        for (int j = 0; j < 6; j++) acc[j] += __ldcg(&partials[b * 8 + j]);
+    for (int j = 0; j < 6; j++) acc[j] = warp_sum(acc[j]);
+    __syncthreads();
+    if (lane == 0)
+        for (int j = 0; j < 6; j++) sh[warp][j] = acc[j];
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double t = 0;
+        for (int w = 0; w < (int)(RED_BLK / 32); w++) t += sh[w][threadIdx.x];
+        out[threadIdx.x] = t;
+    }
+    if (threadIdx.x == 0) *ticket = 0u;
+}
+
+// ------------------------------------------------------------ launchers
+static inline unsigned blocks_for(uint64_t n) { return (unsigned)((n + BLK - 1) / BLK); }
+
+template <class F>
+static cudaError_t dispatch(int storage, F &&fn) {
+    switch (storage) {
+        case 0: return fn((float *)nullptr);
+        case 1: return fn((__half *)nullptr);
+        case 2: return fn((__nv_bfloat16 *)nullptr);
+        case 3: return fn((double *)nullptr);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch27_init(int storage, const LevelParams &p, cudaStream_t st) {
+    return dispatch(storage, [&](auto *t) {
+        using S = std::remove_pointer_t<decltype(t)>;
+        k27_init<S><<<blocks_for(p.N), BLK, 0, st>>>(p);
+        return cudaGetLastError();
+    });
+}
+
+cudaError_t launch27_face(int storage, const LevelParams &p, const StepArgs &a, cudaStream_t st) {
+    if (!p.nface) return cudaSuccess;
+    return dispatch(storage, [&](auto *t) {
+        using S = std::remove_pointer_t<decltype(t)>;
+        k27_face<S><<<blocks_for(p.nface), BLK, 0, st>>>(p, a);
+        return cudaGetLastError();
+    });
+}
+
+cudaError_t launch27_step(int storage, const LevelParams &p, const StepArgs &a, cudaStream_t st) {
+    return dispatch(storage, [&](auto *t) {
+        using S = std::remove_pointer_t<decltype(t)>;
+        if (p.forcing) k27_step<S, true><<<blocks_for(p.N), BLK, 0, st>>>(p, a);
+        else k27_step<S, false><<<blocks_for(p.N), BLK, 0, st>>>(p, a);
+        return cudaGetLastError();
+    });
+}
+
+cudaError_t launch27_ghost(int storage, const LevelParams &p, const StepArgs &a, cudaStream_t st) {
+    if (!p.nghost) return cudaSuccess;
+    return dispatch(storage, [&](auto *t) {
+        using S = std::remove_pointer_t<decltype(t)>;
+        k27_ghost<S><<<blocks_for(p.nghost), BLK, 0, st>>>(p, a);
+        return cudaGetLastError();
+    });
+}
+
+cudaError_t launch27_restrict(int storage, const LevelParams &p, const StepArgs &a, cudaStream_t st) {
+    if (!p.nrestrict) return cudaSuccess;
+    return dispatch(storage, [&](auto *t) {
+        using S = std::remove_pointer_t<decltype(t)>;
+        k27_restrict<S><<<blocks_for(p.nrestrict), BLK, 0, st>>>(p, a);
+        return cudaGetLastError();
+    });
+}
+
+cudaError_t launch27_dump(int storage, const LevelParams &p, uint32_t src, cudaStream_t st) {
+    return dispatch(storage, [&](auto *t) {
+        using S = std::remove_pointer_t<decltype(t)>;
+        k27_dump<S><<<blocks_for(p.N), BLK, 0, st>>>(p, src);
+        return cudaGetLastError();
+    });
+}
+
+cudaError_t launch27_mass(int storage, const LevelParams &p, uint32_t src, double *mass, unsigned long long *bad, cudaStream_t st) {
+    return dispatch(storage, [&](auto *t) {
+        using S = std::remove_pointer_t<decltype(t)>;
+        k27_mass<S><<<blocks_for(p.N), BLK, 0, st>>>(p, src, mass, bad);
+        return cudaGetLastError();
+    });
+}
+
+uint32_t reduce27_blocks(uint32_t nrec) { return (nrec + RED_BLK - 1) / RED_BLK; }
+
+cudaError_t launch27_reduce(const LevelParams &p, int fp64, double *partials, uint32_t *ticket, double *out, cudaStream_t st) {
+    if (p.nrec == 0) return cudaMemsetAsync(out, 0, 6 * sizeof(double), st);
+    const uint32_t nb = reduce27_blocks(p.nrec);
+    if (fp64) k27_reduce<true><<<nb, RED_BLK, 0, st>>>(p, partials, ticket, out);
+    else k27_reduce<false><<<nb, RED_BLK, 0, st>>>(p, partials, ticket, out);
+    return cudaGetLastError();
+}
+
+}  // namespace lbm27

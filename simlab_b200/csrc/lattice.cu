@@ -60,6 +60,11 @@ size_t storage_bytes(int s) { return s == LBM_STORAGE_FP32 ? 4 : (s == LBM_STORA
 
 }  // namespace
 
+// creation errors of the other handle types land in the same message
+namespace lbm_host {
+void set_global_error(const std::string &msg) { g_error = msg; }
+}  // namespace lbm_host
+
 struct lbm_lattice {
     lbm_setup setup{};
     lbm::LatParams lp{};

@@ -33,8 +33,10 @@ def test_struct_layouts_match_the_c_compiler(tmp_path):
     """ctypes mirrors of the C structs have the C compiler's sizes and offsets."""
     import subprocess
 
+    from simlab_b200 import mlattice
+
     structs = {"lbm_setup": lbm._Setup, "lbm_geometry": lbm._Geometry, "lbm_probes": lbm._Probes, "lbm_slice_def": lbm._SliceDef,
-               "lbm_info": lbm._Info}
+               "lbm_info": lbm._Info, "lbm_multi_setup": mlattice._MultiSetup, "lbm_level_box": mlattice._LevelBox}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "simlab_lbm.h"', "int main(void) {"]
     for cname, cls in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
@@ -63,6 +65,23 @@ def test_setup_validation_errors_match_reference():
         lbm.Lattice(LatticeSetup(dims=[8, 8, 8], faces=[FaceBc.PERIODIC, FaceBc.OPEN] + [FaceBc.PERIODIC] * 4))
     with pytest.raises(LbmError, match="out of range"):
         lbm.Lattice(LatticeSetup(dims=[70000, 70000, 3]))
+
+
+def test_multi_setup_validation_errors_match_reference():
+    """mlattice.rs:198-216: nesting and periodic checks, before any device work."""
+    from simlab_b200.mlattice import LevelBox, MultiLattice, MultiSetup
+
+    base = dict(dims0=[64, 48, 48], faces=[FaceBc.VELOCITY] + [FaceBc.OPEN] * 5, nu0=0.01)
+    with pytest.raises(LbmError, match="refinement box 1 does not fit inside its parent"):
+        MultiLattice(MultiSetup(boxes=[LevelBox(lo=[1, 12, 12], n=[32, 24, 24])], **base))
+    with pytest.raises(LbmError, match="refinement box 1 does not fit inside its parent"):
+        MultiLattice(MultiSetup(boxes=[LevelBox(lo=[16, 12, 12], n=[7, 24, 24])], **base))
+    with pytest.raises(LbmError, match="refinement box 2 does not fit inside its parent"):
+        MultiLattice(MultiSetup(boxes=[LevelBox(lo=[16, 12, 12], n=[32, 24, 24]), LevelBox(lo=[2, 10, 10], n=[20, 20, 20])], **base))
+    with pytest.raises(LbmError, match="periodic faces only work without refinement"):
+        MultiLattice(MultiSetup(dims0=[64, 48, 48], faces=[FaceBc.PERIODIC] * 6, nu0=0.01, boxes=[LevelBox(lo=[16, 12, 12], n=[32, 24, 24])]))
+    with pytest.raises(LbmError, match="free-slip"):
+        MultiLattice(MultiSetup(dims0=[16, 16, 16], faces=[FaceBc.FREE_SLIP] * 6, nu0=0.01))
 
 
 def test_max_cells():

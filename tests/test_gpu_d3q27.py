@@ -1,0 +1,160 @@
+"""Multi-level D3Q27 engine (through the C ABI) against the CPU oracle and
+the reference's known answers for the refined solver.  Tolerances: FP32
+relative L2 of the velocity <= 1e-5 on every level (the reference's FP32
+update restated); FP64 engine vs FP64 oracle forces <= 1e-10 relative;
+stochastic-rounding FP16/BF16 storage against the oracle with the same
+storage within the rounding noise (FP16 <= 2e-3, BF16 <= 2e-2 relative L2 of
+the velocity deviation from the free stream)."""
+import numpy as np
+import pytest
+
+from oracle import OracleMulti
+from simlab_b200.lbm import FaceBc, Storage, steps_array, voxelize_static
+from simlab_b200.mlattice import LevelBox, MultiLattice, MultiSetup
+from simlab_b200.shapes import sphere
+
+from helpers import rel_l2
+from test_oracle_d3q27 import check_uniform, momentum27, poiseuille27, uniform_refined_setup
+
+pytestmark = pytest.mark.gpu
+
+UINF = np.array([0.05, 0.004, 0.0])
+
+
+def feature_single(storage=Storage.FP32):
+    """Every single-level feature: Bouzidi sphere, Smagorinsky, sponges with
+    absorbing layer, total-pressure inlet, open faces, body force."""
+    dims = (40, 30, 24)
+    c = (14.3, 15.2, 11.7)
+    v, t = sphere(list(c), 5.3, 4)
+    vox = voxelize_static(v, t, list(dims), 27)
+    F = FaceBc
+    s = MultiSetup(dims0=list(dims), faces=[F.VELOCITY, F.OPEN, F.OPEN, F.OPEN, F.OPEN, F.OPEN], nu0=0.004, smagorinsky=0.17,
+                   u_inf=list(UINF), u_init=[0.04, 0.0, 0.002], body_force0=[1e-6, 0.0, -2e-7], sponge=[4, 6, 3, 3, 0, 2], sponge_tau=0.9,
+                   sponge_sigma=0.1, absorb_velocity=True, total_pressure_inlet=True, storage=storage, center=list(c), debug_dump=True)
+    return s, vox
+
+
+def feature_multi(storage=Storage.FP32):
+    """Three levels, the sphere on the finest; open faces with a velocity inlet."""
+    F = FaceBc
+    s = MultiSetup(dims0=[48, 36, 36], faces=[F.VELOCITY] + [F.OPEN] * 5, nu0=0.02, smagorinsky=0.1, u_inf=list(UINF),
+                   u_init=[0.04, 0.0, 0.002], sponge=[0, 6, 0, 0, 0, 0], sponge_tau=0.9, sponge_sigma=0.05, total_pressure_inlet=True,
+                   storage=storage, debug_dump=True)
+    s.boxes = [LevelBox(lo=[12, 9, 9], n=[16, 14, 14]), LevelBox(lo=[8, 7, 7], n=[10, 8, 8])]
+    c = [9.3, 7.2, 7.1]
+    s.center = c
+    v, t = sphere(c, 3.5, 4)
+    vox = voxelize_static(v, t, list(s.dims(2)), 27)
+    return s, vox
+
+
+def spin(n, w=(0.0, 0.0, 0.003)):
+    a = steps_array(n)
+    a["omega"] = np.asarray(w)
+    return a
+
+
+def _u(m):
+    return np.asarray(m)[:, 1:4].astype(np.float64)
+
+
+def test_init_and_records_match_oracle():
+    s, vox = feature_single()
+    g, o = MultiLattice(s, vox), OracleMulti(s, vox)
+    assert g.level_dims() == o.level_dims()
+    mg, mo = g.macros(0), o.macros(0)
+    assert np.array_equal(np.isnan(mg[:, 0]), np.isnan(mo[:, 0]))
+    assert rel_l2(_u(mg), _u(mo)) < 1e-6
+    assert np.array_equal(g.records(), o.records())
+
+
+def test_single_level_fp32_parity():
+    s, vox = feature_single()
+    g, o = MultiLattice(s, vox), OracleMulti(s, vox)
+    hg, ho = g.run(spin(150)), o.run(spin(150))
+    mg, mo = g.macros(0), o.macros(0)
+    assert np.array_equal(np.isnan(mg[:, 0]), np.isnan(mo[:, 0]))
+    assert rel_l2(_u(mg), _u(mo)) <= 1e-5
+    assert rel_l2(mg[:, 0], mo[:, 0]) <= 1e-6
+    assert np.max(np.abs(hg - ho)) <= 1e-5 * np.max(np.abs(ho))
+    rg, ro = g.records().reshape(-1, 24), o.records().reshape(-1, 24)
+    assert np.array_equal(rg[:, :15], ro[:, :15])
+    fg, fo = rg[:, 15:21].view(np.float32), ro[:, 15:21].view(np.float32)
+    assert np.max(np.abs(fg - fo)) <= 1e-5 * np.max(np.abs(fo))
+
+
+def test_three_levels_fp32_parity():
+    s, vox = feature_multi()
+    g, o = MultiLattice(s, vox), OracleMulti(s, vox)
+    assert g.sub_steps() == 4
+    hg, ho = g.run(spin(120)), o.run(spin(120))
+    for l in range(3):
+        mg, mo = g.macros(l), o.macros(l)
+        assert np.array_equal(np.isnan(mg[:, 0]), np.isnan(mo[:, 0])), l
+        assert rel_l2(_u(mg), _u(mo)) <= 1e-5, l
+    assert np.max(np.abs(hg - ho)) <= 1e-5 * np.max(np.abs(ho))
+
+
+def test_fp64_engine_matches_fp64_oracle():
+    s, vox = feature_multi(Storage.FP64)
+    g, o = MultiLattice(s, vox), OracleMulti(s, vox, real64=True)
+    hg, ho = g.run(spin(80)), o.run(spin(80))
+    assert np.max(np.abs(hg - ho)) <= 1e-10 * np.max(np.abs(ho))
+    for l in range(3):
+        assert rel_l2(_u(g.macros(l)), _u(o.macros(l))) < 1e-6
+
+
+@pytest.mark.parametrize("storage,tol", [(Storage.FP16, 2e-3), (Storage.BF16, 2e-2)])
+def test_reduced_storage_parity(storage, tol):
+    s, vox = feature_multi(storage)
+    g, o = MultiLattice(s, vox), OracleMulti(s, vox)
+    hg, ho = g.run(80), o.run(80)
+    for l in range(3):
+        ug, uo = _u(g.macros(l)), _u(o.macros(l))
+        assert rel_l2(ug - UINF, uo - UINF) <= tol, l
+    assert abs(hg[-1, 0] / ho[-1, 0] - 1.0) < 10 * tol
+
+
+def test_gpu_d3q27_poiseuille_second_order():
+    """refined.rs:67-81 on the engine."""
+    e = []
+    for h in (8.0, 16.0, 32.0):
+        err, bal = poiseuille27(h, MultiLattice)
+        assert abs(bal) < 1e-3
+        e.append(err)
+    assert np.log2(e[1] / e[2]) > 1.7 and e[2] < 1e-3
+
+
+def test_gpu_d3q27_momentum_balance():
+    assert abs(momentum27(MultiLattice)) < 1e-3
+
+
+def test_gpu_uniform_stream_crosses_refinement_unchanged():
+    lat = MultiLattice(uniform_refined_setup())
+    lat.run(100 * lat.sub_steps())
+    check_uniform(lat)
+
+
+def test_gpu_step_count_must_be_a_multiple():
+    from simlab_b200.lbm import LbmError
+
+    lat = MultiLattice(uniform_refined_setup())
+    with pytest.raises(LbmError, match="multiple of 4"):
+        lat.run(6)
+
+
+def test_mass_conserved_with_halfway_walls():
+    """A periodic box with a halfway-walled sphere conserves mass to round-off."""
+    from simlab_b200.lbm import halfway
+
+    n = 24
+    v, t = sphere([12.3, 11.4, 12.17], 4.0, 4)
+    vox = halfway(voxelize_static(v, t, [n, n, n], 27))
+    s = MultiSetup(dims0=[n, n, n], faces=[FaceBc.PERIODIC] * 6, nu0=0.05, u_inf=[0.03, 0, 0], u_init=[0.03, 0, 0])
+    g = MultiLattice(s, vox)
+    m0, b0 = g.mass(0)
+    g.run(200)
+    m1, b1 = g.mass(0)
+    assert b0 == 0 and b1 == 0
+    assert abs(m1 / m0 - 1.0) < 1e-6
