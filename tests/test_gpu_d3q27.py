@@ -144,17 +144,20 @@ def test_gpu_step_count_must_be_a_multiple():
         lat.run(6)
 
 
-def test_mass_conserved_with_halfway_walls():
-    """A periodic box with a halfway-walled sphere conserves mass to round-off."""
+@pytest.mark.parametrize("storage,tol", [(Storage.FP64, 1e-8), (Storage.FP32, 5e-6)])
+def test_mass_conserved_with_halfway_walls(storage, tol):
+    """A periodic box with a halfway-walled sphere conserves mass: to 1e-8 in
+    FP64; in FP32 the cumulant transforms round with a small bias (the FP32
+    oracle drifts by 1.5e-6 over these 200 steps as well)."""
     from simlab_b200.lbm import halfway
 
     n = 24
     v, t = sphere([12.3, 11.4, 12.17], 4.0, 4)
     vox = halfway(voxelize_static(v, t, [n, n, n], 27))
-    s = MultiSetup(dims0=[n, n, n], faces=[FaceBc.PERIODIC] * 6, nu0=0.05, u_inf=[0.03, 0, 0], u_init=[0.03, 0, 0])
+    s = MultiSetup(dims0=[n, n, n], faces=[FaceBc.PERIODIC] * 6, nu0=0.05, u_inf=[0.03, 0, 0], u_init=[0.03, 0, 0], storage=storage)
     g = MultiLattice(s, vox)
     m0, b0 = g.mass(0)
     g.run(200)
     m1, b1 = g.mass(0)
     assert b0 == 0 and b1 == 0
-    assert abs(m1 / m0 - 1.0) < 1e-6
+    assert abs(m1 / m0 - 1.0) < tol
