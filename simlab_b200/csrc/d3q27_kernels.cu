@@ -177,84 +177,6 @@ __device__ __forceinline__ void rebuild(R rho, const R *u, const R *pp, R *f) {
     fneq_add<R>(d, f);
 }
 
-// one backward central-moment transform along an axis (mshader.rs:316-322):
-// central moments (k0, k1, k2) about velocity w -> populations (-1, 0, +1)
-template <class R>
-__device__ __forceinline__ void back(R k0, R k1, R k2, R w, R &m, R &o, R &pl) {
-    const R r1 = k1 + w * k0;
-    const R r2 = k2 + (R)2 * w * k1 + w * w * k0;
-    m = (R)0.5 * (r2 - r1);
-    o = k0 - r2;
-    pl = (R)0.5 * (r2 + r1);
-}
-// the same with k1 = 0 (the odd central moments that vanish without forcing)
-template <class R>
-__device__ __forceinline__ void back0(R k0, R k2, R w, R &m, R &o, R &pl) {
-    const R r1 = w * k0;
-    const R r2 = k2 + w * w * k0;
-    m = (R)0.5 * (r2 - r1);
-    o = k0 - r2;
-    pl = (R)0.5 * (r2 + r1);
-}
-// the same with k0 = k2 = 0
-template <class R>
-__device__ __forceinline__ void back_odd(R k1, R w, R &m, R &o, R &pl) {
-    const R r1 = k1;
-    const R r2 = (R)2 * w * k1;
-    m = (R)0.5 * (r2 - r1);
-    o = -r2;
-    pl = (R)0.5 * (r2 + r1);
-}
-
-// mshader.rs:286-362: populations (shifted) of the Gaussian with covariance
-// sg (xx yy zz xy xz yz) and first central moments m1, higher cumulants zero
-template <class R, bool FORCE>
-__device__ __forceinline__ void gauss(R rho, const R *u, const R *sg, const R *m1, R *f) {
-    const R a = sg[0], b = sg[1], cc = sg[2], d = sg[3], e = sg[4], g = sg[5];
-    const R two = 2;
-    // z pass: Z[i][j][cz] from k_ij0, k_ij1, k_ij2
-    R Z[3][3][3];
-    const R k000 = rho, k200 = rho * a, k020 = rho * b, k002 = rho * cc, k110 = rho * d, k101 = rho * e, k011 = rho * g;
-    const R k220 = rho * (a * b + two * d * d), k202 = rho * (a * cc + two * e * e), k022 = rho * (b * cc + two * g * g);
-    const R k211 = rho * (a * g + two * d * e), k121 = rho * (b * e + two * d * g), k112 = rho * (cc * d + two * e * g);
-    const R k222 = rho * (a * b * cc + two * (a * g * g + b * e * e + cc * d * d) + (R)8 * d * e * g);
-    const R w = u[2];
-    if (FORCE) {
-        const R k100 = rho * m1[0], k010 = rho * m1[1], k001 = rho * m1[2];
-        back<R>(k000, k001, k002, w, Z[0][0][0], Z[0][0][1], Z[0][0][2]);
-        back<R>(k100, k101, (R)0, w, Z[1][0][0], Z[1][0][1], Z[1][0][2]);
-        back<R>(k010, k011, (R)0, w, Z[0][1][0], Z[0][1][1], Z[0][1][2]);
-    } else {
-        back0<R>(k000, k002, w, Z[0][0][0], Z[0][0][1], Z[0][0][2]);
-        back_odd<R>(k101, w, Z[1][0][0], Z[1][0][1], Z[1][0][2]);
-        back_odd<R>(k011, w, Z[0][1][0], Z[0][1][1], Z[0][1][2]);
-    }
-    back0<R>(k200, k202, w, Z[2][0][0], Z[2][0][1], Z[2][0][2]);
-    back0<R>(k110, k112, w, Z[1][1][0], Z[1][1][1], Z[1][1][2]);
-    back_odd<R>(k211, w, Z[2][1][0], Z[2][1][1], Z[2][1][2]);
-    back0<R>(k020, k022, w, Z[0][2][0], Z[0][2][1], Z[0][2][2]);
-    back_odd<R>(k121, w, Z[1][2][0], Z[1][2][1], Z[1][2][2]);
-    back0<R>(k220, k222, w, Z[2][2][0], Z[2][2][1], Z[2][2][2]);
-    // y pass: Y[i][cz][cy]
-    R Y[3][3][3];
-#pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int c = 0; c < 3; c++) back<R>(Z[i][0][c], Z[i][1][c], Z[i][2][c], u[1], Y[i][c][0], Y[i][c][1], Y[i][c][2]);
-    // x pass: f(cx, cy, cz)
-#pragma unroll
-    for (int cyi = 0; cyi < 3; cyi++)
-#pragma unroll
-        for (int czi = 0; czi < 3; czi++) {
-            R m, o, pl;
-            back<R>(Y[0][czi][cyi], Y[1][czi][cyi], Y[2][czi][cyi], u[0], m, o, pl);
-            const int base = 3 * cyi + 9 * czi;  // direction of (cx = -1, cy, cz)
-            f[base] = m - W<R>(base);
-            f[base + 1] = o - W<R>(base + 1);
-            f[base + 2] = pl - W<R>(base + 2);
-        }
-}
-
 template <class R>
 __device__ __forceinline__ R sponge(const LevelParams &p, const Consts27<R> &k, uint32_t x, uint32_t y, uint32_t z) {
     const R pp[3] = {(R)(float)x, (R)(float)y, (R)(float)z};
@@ -276,36 +198,166 @@ __device__ __forceinline__ Rng cell_rng(uint32_t n, uint32_t seed_mix) {
 }
 
 // ------------------------------------------------------------ the step
-template <class S, bool FORCE>
-__global__ void __launch_bounds__(BLK) k27_step(const __grid_constant__ LevelParams p, const StepArgs a) {
+// Storage in raw units: FP16 keeps (f - w) * 32768, the others f - w.  The
+// step works on raw loads (no per-population rescale), scales the moments
+// once, and folds the scale back into the last multiply of each output.
+// Stochastic rounding takes two noise fields from each generator step.
+template <class S> struct Raw;
+template <> struct Raw<float> {
+    static constexpr float SC = 1.0f;
+    static __device__ __forceinline__ float ld(const float *p) { return *p; }
+    static __device__ __forceinline__ void st2(float *a, float va, float *b, float vb, Rng &) { *a = va; *b = vb; }
+    static __device__ __forceinline__ void st1(float *a, float va, Rng &) { *a = va; }
+};
+template <> struct Raw<double> {
+    static constexpr double SC = 1.0;
+    static __device__ __forceinline__ double ld(const double *p) { return *p; }
+    static __device__ __forceinline__ void st2(double *a, double va, double *b, double vb, Rng &) { *a = va; *b = vb; }
+    static __device__ __forceinline__ void st1(double *a, double va, Rng &) { *a = va; }
+};
+template <> struct Raw<__half> {
+    static constexpr float SC = 32768.0f;
+    static __device__ __forceinline__ float ld(const __half *p) { return __half2float(*p); }
+    // 13 random bits below binary16's mantissa, then round toward zero
+    static __device__ __forceinline__ void st2(__half *a, float va, __half *b, float vb, Rng &r) {
+        const uint32_t x = r.next();
+        *a = __float2half_rz(__uint_as_float(__float_as_uint(va) + (x >> 19)));
+        *b = __float2half_rz(__uint_as_float(__float_as_uint(vb) + ((x >> 6) & 0x1fffu)));
+    }
+    static __device__ __forceinline__ void st1(__half *a, float va, Rng &r) {
+        *a = __float2half_rz(__uint_as_float(__float_as_uint(va) + (r.next() >> 19)));
+    }
+};
+template <> struct Raw<__nv_bfloat16> {
+    static constexpr float SC = 1.0f;
+    static __device__ __forceinline__ float ld(const __nv_bfloat16 *p) { return __bfloat162float(*p); }
+    // 16 random bits below bfloat16's mantissa, then truncate
+    static __device__ __forceinline__ void st2(__nv_bfloat16 *a, float va, __nv_bfloat16 *b, float vb, Rng &r) {
+        const uint32_t x = r.next();
+        *a = __ushort_as_bfloat16((unsigned short)((__float_as_uint(va) + (x >> 16)) >> 16));
+        *b = __ushort_as_bfloat16((unsigned short)((__float_as_uint(vb) + (x & 0xffffu)) >> 16));
+    }
+    static __device__ __forceinline__ void st1(__nv_bfloat16 *a, float va, Rng &r) {
+        *a = __ushort_as_bfloat16((unsigned short)((__float_as_uint(va) + (r.next() >> 16)) >> 16));
+    }
+};
+
+// backward transforms with the factor 1/2 of the outer two outputs deferred:
+// returns (2 f-, f0, 2 f+) of mshader.rs:316-322; w2 = 2 w, ww = w^2
+template <class R>
+__device__ __forceinline__ void bk(R k0, R k1, R k2, R w, R w2, R ww, R &m, R &o, R &pl) {
+    const R r1 = k1 + w * k0;
+    const R r2 = k2 + w2 * k1 + ww * k0;
+    m = r2 - r1; o = k0 - r2; pl = r2 + r1;
+}
+template <class R>  // k1 = 0
+__device__ __forceinline__ void bk_even(R k0, R k2, R w, R ww, R &m, R &o, R &pl) {
+    const R r1 = w * k0;
+    const R r2 = k2 + ww * k0;
+    m = r2 - r1; o = k0 - r2; pl = r2 + r1;
+}
+template <class R>  // k0 = k2 = 0
+__device__ __forceinline__ void bk_odd(R k1, R w2, R &m, R &o, R &pl) {
+    const R r2 = w2 * k1;
+    m = r2 - k1; o = -r2; pl = r2 + k1;
+}
+
+// The Gaussian's populations (mshader.rs:286-362) with rho factored out of
+// every central moment and the halves deferred: output (cx, cy, cz) carries
+// the factor 2^(|cx|+|cy|+|cz|), removed with rho and the storage scale in
+// the final multiply-add emit(i, X * rs[|c|] - SC w_i).
+template <class R, bool FORCE, class Emit>
+__device__ __forceinline__ void gauss_raw(const R *u, const R *sg, const R *m1, const R *rs, R SC, Emit &&emit) {
+    const R a = sg[0], b = sg[1], cc = sg[2], d = sg[3], e = sg[4], g = sg[5];
+    const R two = 2;
+    const R k220 = a * b + two * d * d, k202 = a * cc + two * e * e, k022 = b * cc + two * g * g;
+    const R k211 = a * g + two * d * e, k121 = b * e + two * d * g, k112 = cc * d + two * e * g;
+    const R k222 = a * b * cc + two * (a * g * g + b * e * e + cc * d * d) + (R)8 * d * e * g;
+    R w2[3], ww[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) { w2[c] = two * u[c]; ww[c] = u[c] * u[c]; }
+    R Z[3][3][3];
+    const R wz = u[2];
+    if (FORCE) {
+        bk<R>((R)1, m1[2], cc, wz, w2[2], ww[2], Z[0][0][0], Z[0][0][1], Z[0][0][2]);
+        bk<R>(m1[0], e, (R)0, wz, w2[2], ww[2], Z[1][0][0], Z[1][0][1], Z[1][0][2]);
+        bk<R>(m1[1], g, (R)0, wz, w2[2], ww[2], Z[0][1][0], Z[0][1][1], Z[0][1][2]);
+    } else {
+        bk_even<R>((R)1, cc, wz, ww[2], Z[0][0][0], Z[0][0][1], Z[0][0][2]);
+        bk_odd<R>(e, w2[2], Z[1][0][0], Z[1][0][1], Z[1][0][2]);
+        bk_odd<R>(g, w2[2], Z[0][1][0], Z[0][1][1], Z[0][1][2]);
+    }
+    bk_even<R>(a, k202, wz, ww[2], Z[2][0][0], Z[2][0][1], Z[2][0][2]);
+    bk_even<R>(d, k112, wz, ww[2], Z[1][1][0], Z[1][1][1], Z[1][1][2]);
+    bk_odd<R>(k211, w2[2], Z[2][1][0], Z[2][1][1], Z[2][1][2]);
+    bk_even<R>(b, k022, wz, ww[2], Z[0][2][0], Z[0][2][1], Z[0][2][2]);
+    bk_odd<R>(k121, w2[2], Z[1][2][0], Z[1][2][1], Z[1][2][2]);
+    bk_even<R>(k220, k222, wz, ww[2], Z[2][2][0], Z[2][2][1], Z[2][2][2]);
+    R Y[3][3][3];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) bk<R>(Z[i][0][c], Z[i][1][c], Z[i][2][c], u[1], w2[1], ww[1], Y[i][c][0], Y[i][c][1], Y[i][c][2]);
+#pragma unroll
+    for (int cyi = 0; cyi < 3; cyi++)
+#pragma unroll
+        for (int czi = 0; czi < 3; czi++) {
+            R m, o, pl;
+            bk<R>(Y[0][czi][cyi], Y[1][czi][cyi], Y[2][czi][cyi], u[0], w2[0], ww[0], m, o, pl);
+            const int base = 3 * cyi + 9 * czi;  // direction (cx = -1, cy, cz)
+            const int nz = (cyi != 1) + (czi != 1);
+            emit(base, m * rs[nz + 1] - SC * W<R>(base));
+            emit(base + 1, o * rs[nz] - SC * W<R>(base + 1));
+            emit(base + 2, pl * rs[nz + 1] - SC * W<R>(base + 2));
+        }
+}
+
+// Register budget (blocks of 256 threads per SM): FP32/FP16/BF16 without
+// periodic wrap run 3 (80 registers, a few spilled to L1), with wrap 2; the
+// FP64 engine (a validation instrument) keeps the compiler's choice.
+template <class S, bool WRAP> struct StepOcc { static constexpr int value = WRAP ? 2 : 3; };
+template <bool WRAP> struct StepOcc<double, WRAP> { static constexpr int value = 1; };
+
+// WRAP: the level has periodic axes (neighbour offsets per thread); without
+// them no stepped cell touches the boundary, and every neighbour offset is
+// uniform across the grid
+template <class S, bool FORCE, bool WRAP>
+__global__ void __launch_bounds__(BLK, StepOcc<S, WRAP>::value) k27_step(const __grid_constant__ LevelParams p, const StepArgs a) {
     using R = typename Pop<S>::real;
     const uint32_t n = blockIdx.x * BLK + threadIdx.x;
     if (n >= p.N) return;
     const uint32_t fg = p.flags[n];
     if ((fg & 7u) != 0) return;
     const Consts27<R> &k = K<R>(p);
+    const R SC = (R)Raw<S>::SC, ISC = (R)1 / (R)Raw<S>::SC;
     uint32_t x, y, z;
     coords(p, n, x, y, z);
-    // neighbour rows with periodic wrap (mshader.rs:135-138)
-    const uint32_t xi[3] = {x == 0 ? p.NX - 1 : x - 1, x, x == p.NX - 1 ? 0 : x + 1};
-    const uint32_t yi[3] = {y == 0 ? p.NY - 1 : y - 1, y, y == p.NY - 1 ? 0 : y + 1};
-    const uint32_t zi[3] = {z == 0 ? p.NZ - 1 : z - 1, z, z == p.NZ - 1 ? 0 : z + 1};
     const S *src = set_ptr<S>(p, a.src);
+    const S *srcn = src + n;
+    const int64_t NP = (int64_t)p.NP, SX = 1, SY = (int64_t)p.NX, SZ = (int64_t)p.NX * p.NY;
     R f[27];
-    // pull: the population moving along c_i comes from n - c_i
+    if (WRAP) {
+        // offsets of the axis neighbours with periodic wrap (mshader.rs:135-138)
+        const int32_t nx = (int32_t)p.NX, nxy = (int32_t)(p.NX * p.NY);
+        const int32_t xo[3] = {x == 0 ? nx - 1 : -1, 0, x == p.NX - 1 ? -(nx - 1) : 1};
+        const int32_t yo[3] = {y == 0 ? (int32_t)(p.NY - 1) * nx : -nx, 0, y == p.NY - 1 ? -(int32_t)(p.NY - 1) * nx : nx};
+        const int32_t zo[3] = {z == 0 ? (int32_t)(p.NZ - 1) * nxy : -nxy, 0, z == p.NZ - 1 ? -(int32_t)(p.NZ - 1) * nxy : nxy};
 #pragma unroll
-    for (int i = 0; i < 27; i++) {
-        const uint32_t m = (zi[1 - CZ(i)] * p.NY + yi[1 - CY(i)]) * p.NX + xi[1 - CX(i)];
-        f[i] = Pop<S>::ld(src + (uint64_t)i * p.NP + m);
+        for (int i = 0; i < 27; i++) f[i] = Raw<S>::ld(srcn + ((int64_t)i * NP + (xo[1 - CX(i)] + yo[1 - CY(i)] + zo[1 - CZ(i)])));
+    } else {
+        // pull: the population moving along c_i comes from n - c_i
+#pragma unroll
+        for (int i = 0; i < 27; i++) f[i] = Raw<S>::ld(srcn + ((int64_t)i * NP - CX(i) * SX - CY(i) * SY - CZ(i) * SZ));
     }
     const uint32_t rec = fg >> 3;
-    R Fv[3] = {0, 0, 0}, Tv[3] = {0, 0, 0};
     if (rec != 0) {
+        // Bouzidi bounce-back with moving-wall momentum exchange (mshader.rs:364-403)
         const uint32_t r = rec - 1;
         const uint32_t mask = p.recs[r * RS + R_MASK];
         R fin[27];
 #pragma unroll
-        for (int i = 0; i < 27; i++) fin[i] = f[i];
+        for (int i = 0; i < 27; i++) fin[i] = f[i] * ISC;
+        R Fv[3] = {0, 0, 0}, Tv[3] = {0, 0, 0};
         const R pc[3] = {(R)(float)x - k.center[0], (R)(float)y - k.center[1], (R)(float)z - k.center[2]};
         R om[3];
         if (sizeof(R) == 8) { om[0] = (R)a.omega_d[0]; om[1] = (R)a.omega_d[1]; om[2] = (R)a.omega_d[2]; }
@@ -318,8 +370,8 @@ __global__ void __launch_bounds__(BLK) k27_step(const __grid_constant__ LevelPar
             const uint32_t wq = p.recs[r * RS + R_Q + SLOT(i) / 2];
             const uint16_t hq = (SLOT(i) & 1) ? (uint16_t)(wq >> 16) : (uint16_t)(wq & 0xffffu);
             const R q = max((R)__half2float(__ushort_as_half(hq)), (R)0.001f);
-            const R fpi = Pop<S>::ld(src + (uint64_t)i * p.NP + n) + W<R>(i);
-            const R fpo = Pop<S>::ld(src + (uint64_t)o * p.NP + n) + W<R>(i);
+            const R fpi = Raw<S>::ld(srcn + (int64_t)i * NP) * ISC + W<R>(i);
+            const R fpo = Raw<S>::ld(srcn + (int64_t)o * NP) * ISC + W<R>(i);
             const R ci[3] = {(R)CX(i), (R)CY(i), (R)CZ(i)};
             const R xw[3] = {pc[0] + q * ci[0], pc[1] + q * ci[1], pc[2] + q * ci[2]};
             const R uw[3] = {om[1] * xw[2] - om[2] * xw[1], om[2] * xw[0] - om[0] * xw[2], om[0] * xw[1] - om[1] * xw[0]};
@@ -329,7 +381,7 @@ __global__ void __launch_bounds__(BLK) k27_step(const __grid_constant__ LevelPar
             if (q >= (R)0.5) fb = (fpi + ((R)2 * q - (R)1) * fpo - w6 * cu) / ((R)2 * q);
             else if (!(mask & (1u << o))) fb = (R)2 * q * fpi + ((R)1 - (R)2 * q) * (fin[i] + W<R>(i)) - w6 * cu;
             else fb = fpi - w6 * cu;
-            f[o] = fb - W<R>(i);
+            f[o] = (fb - W<R>(i)) * SC;
             R flk[3];
 #pragma unroll
             for (int c = 0; c < 3; c++) flk[c] = (ci[c] - uw[c]) * fpi + (ci[c] + uw[c]) * fb;
@@ -339,8 +391,22 @@ __global__ void __launch_bounds__(BLK) k27_step(const __grid_constant__ LevelPar
             Tv[1] += xw[2] * flk[0] - xw[0] * flk[2];
             Tv[2] += xw[0] * flk[1] - xw[1] * flk[0];
         }
+        for (int c = 0; c < 3; c++) {
+            p.recs[r * RS + R_FT + c] = __float_as_uint((float)Fv[c]);
+            p.recs[r * RS + R_FT + 3 + c] = __float_as_uint((float)Tv[c]);
+        }
+        if (p.recd) {
+            for (int c = 0; c < 3; c++) { p.recd[r * 6 + c] = (double)Fv[c]; p.recd[r * 6 + 3 + c] = (double)Tv[c]; }
+        }
     }
-    const Mom<R> mo = moments<R>(f);
+    Mom<R> mo = moments<R>(f);
+    if (Raw<S>::SC != 1) {
+        mo.rho1 *= ISC;
+#pragma unroll
+        for (int c = 0; c < 3; c++) mo.j[c] *= ISC;
+#pragma unroll
+        for (int c = 0; c < 6; c++) mo.s[c] *= ISC;
+    }
     const R rho = (R)1 + mo.rho1;
     const R inv_rho = (R)1 / rho;
     R G[3] = {0, 0, 0}, u[3];
@@ -367,41 +433,52 @@ __global__ void __launch_bounds__(BLK) k27_step(const __grid_constant__ LevelPar
     const R om1 = (R)1 - (R)1 / tau;
     const R third = (R)1 / (R)3;
     R sg[6];
+    const R om1r = om1 * inv_rho;
 #pragma unroll
-    for (int c = 0; c < 3; c++) sg[c] = third + om1 * dv[c] * inv_rho;
+    for (int c = 0; c < 3; c++) sg[c] = third + om1r * dv[c];
 #pragma unroll
-    for (int c = 3; c < 6; c++) sg[c] = om1 * dv[c] * inv_rho;
+    for (int c = 3; c < 6; c++) sg[c] = om1r * dv[c];
     R m1[3] = {0, 0, 0};
     if (FORCE) {
 #pragma unroll
         for (int c = 0; c < 3; c++) m1[c] = (R)0.5 * G[c] * inv_rho;
     }
-    R fo[27];
-    gauss<R, FORCE>(rho, u, sg, m1, fo);
-    if (p.n_sponge && k.sigma > (R)0 && sp > (R)0) {
-        // absorbing layer: pull density (and with abs_u, velocity) toward the far field
-        R ft[27], fc[27];
-        if (p.abs_u) feq<R>((R)1, k.u_inf[0], k.u_inf[1], k.u_inf[2], ft);
-        else feq<R>((R)1, u[0], u[1], u[2], ft);
-        feq<R>(rho, u[0], u[1], u[2], fc);
-        const R sgm = k.sigma * sp * sp;
-#pragma unroll
-        for (int i = 0; i < 27; i++) fo[i] += sgm * (ft[i] - fc[i]);
-    }
-    if (rec != 0) {
-        const uint32_t r = rec - 1;
+    // absorbing layer (mshader.rs:663-673): fo += sigma sp^2 (feq(1, ut) - feq(rho, u)),
+    // both product-form equilibria, so per direction a product of axis factors
+    const bool absorb = p.n_sponge && k.sigma > (R)0 && sp > (R)0;
+    R at[3][3], ac[3][3], sgm = 0;
+    if (absorb) {
+        const R h = (R)0.5;
+        const R ut[3] = {p.abs_u ? k.u_inf[0] : u[0], p.abs_u ? k.u_inf[1] : u[1], p.abs_u ? k.u_inf[2] : u[2]};
 #pragma unroll
         for (int c = 0; c < 3; c++) {
-            p.recs[r * RS + R_FT + c] = __float_as_uint((float)Fv[c]);
-            p.recs[r * RS + R_FT + 3 + c] = __float_as_uint((float)Tv[c]);
+            const R tt = ut[c] * ut[c], uu = u[c] * u[c];
+            at[c][0] = h * (third + tt - ut[c]); at[c][1] = (R)2 / (R)3 - tt; at[c][2] = h * (third + tt + ut[c]);
+            ac[c][0] = h * (third + uu - u[c]); ac[c][1] = (R)2 / (R)3 - uu; ac[c][2] = h * (third + uu + u[c]);
         }
-        if (p.recd) {
-#pragma unroll
-            for (int c = 0; c < 3; c++) { p.recd[r * 6 + c] = (double)Fv[c]; p.recd[r * 6 + 3 + c] = (double)Tv[c]; }
-        }
+        sgm = k.sigma * sp * sp * SC;
     }
+    const R rs[4] = {rho * SC, rho * SC * (R)0.5, rho * SC * (R)0.25, rho * SC * (R)0.125};
     Rng rng = cell_rng<S>(n, a.seed_mix);
-    put<S>(p, 1u - a.src, n, fo, rng);
+    S *dstn = set_ptr_w<S>(p, 1u - a.src) + n;
+    R pend = 0;
+    int pend_i = -1;
+    gauss_raw<R, FORCE>(u, sg, m1, rs, SC, [&](int i, R v) {
+        if (absorb) {
+            const int ix = CX(i) + 1, iy = CY(i) + 1, iz = CZ(i) + 1;
+            v += sgm * (at[0][ix] * at[1][iy] * at[2][iz] - rho * ac[0][ix] * ac[1][iy] * ac[2][iz]);
+        }
+        // stores go out in pairs (in emission order) so one generator step
+        // rounds two values; the indices are compile-time after unrolling
+        if (pend_i < 0) {
+            pend = v;
+            pend_i = i;
+        } else {
+            Raw<S>::st2(dstn + (int64_t)pend_i * NP, pend, dstn + (int64_t)i * NP, v, rng);
+            pend_i = -1;
+        }
+    });
+    if (pend_i >= 0) Raw<S>::st1(dstn + (int64_t)pend_i * NP, pend, rng);
     // moments for the finer level's ghosts (child box surface)
     if (p.has_child) {
         const int lx = (int)x - p.ch_lo[0], ly = (int)y - p.ch_lo[1], lz = (int)z - p.ch_lo[2];
@@ -683,8 +760,14 @@ cudaError_t launch27_face(int storage, const LevelParams &p, const StepArgs &a, 
 cudaError_t launch27_step(int storage, const LevelParams &p, const StepArgs &a, cudaStream_t st) {
     return dispatch(storage, [&](auto *t) {
         using S = std::remove_pointer_t<decltype(t)>;
-        if (p.forcing) k27_step<S, true><<<blocks_for(p.N), BLK, 0, st>>>(p, a);
-        else k27_step<S, false><<<blocks_for(p.N), BLK, 0, st>>>(p, a);
+        const bool wrap = p.per[0] || p.per[1] || p.per[2];
+        if (p.forcing) {
+            if (wrap) k27_step<S, true, true><<<blocks_for(p.N), BLK, 0, st>>>(p, a);
+            else k27_step<S, true, false><<<blocks_for(p.N), BLK, 0, st>>>(p, a);
+        } else {
+            if (wrap) k27_step<S, false, true><<<blocks_for(p.N), BLK, 0, st>>>(p, a);
+            else k27_step<S, false, false><<<blocks_for(p.N), BLK, 0, st>>>(p, a);
+        }
         return cudaGetLastError();
     });
 }
