@@ -336,6 +336,68 @@ int lbm_multi_get_info(const lbm_multi *h, lbm_info *out);
  * (no reference counterpart). */
 int lbm_multi_mass(lbm_multi *h, uint32_t level, double *mass, uint64_t *nonfinite);
 
+/* ------------------------------------------------------------------------
+ * Gray-level lattice and its discrete adjoint (no counterpart in the
+ * reference, which has no adjoint and no gray level).  A D3Q19 BGK lattice
+ * whose cells carry a solid fraction gamma in [0, 1]; a cell removes the
+ * fraction a = alpha * gamma of its momentum each step (Brinkman drag, added
+ * to BGK with the exact-difference method: the post-collision state gains
+ * feq(rho, (1 - a) u) - feq(rho, u)).  Faces: equilibrium velocity inlet at
+ * -x, zero-gradient outlet at +x (the outlet cell copies its inner
+ * neighbour), periodic in y and z.  The force on the gray body is the
+ * momentum it removes, sum over cells of a * j; its moment is taken about
+ * `center`.
+ *
+ * lbm_backward gives d(objective)/d(gamma) for every design-box cell by a
+ * hand-written discrete adjoint of the whole step (faces, pull streaming,
+ * collision, objective), with checkpoints of the full state every
+ * checkpoint_every steps and the forward recomputed segment by segment.
+ * ------------------------------------------------------------------------ */
+typedef struct {
+    uint32_t dims[3];
+    uint32_t box_lo[3];         /* design box: first cell and size per axis */
+    uint32_t box_n[3];
+    int32_t storage;            /* LBM_STORAGE_FP32 or LBM_STORAGE_FP64 */
+    double nu;                  /* lattice viscosity, tau = 0.5 + 3 nu */
+    double u_in[3];             /* inlet velocity (and initial state) */
+    double alpha;               /* momentum fraction removed per step at gamma = 1 (0 < alpha <= 1) */
+    double center[3];           /* moment reference */
+} lbm_gray_setup;
+
+/* The objective: J = mean over steps t0..t1 (1-based, inclusive) of
+ * dir . F_t (objective 0) or dir . M_t (objective 1), F_t and M_t the force
+ * and moment on the gray body after step t. */
+typedef struct {
+    uint64_t steps;             /* forward steps from the initial state */
+    uint64_t t0, t1;
+    uint32_t checkpoint_every;  /* full-state checkpoint interval */
+    int32_t objective;          /* 0 force, 1 moment */
+    double dir[3];
+    int32_t recompute;          /* 1: recompute every segment from its checkpoint; 0: keep the
+                                   per-step moments of the first pass when they fit in HBM */
+    int32_t _pad;
+} lbm_adjoint_spec;
+
+typedef struct lbm_gray lbm_gray;
+
+int lbm_gray_create(const lbm_gray_setup *setup, lbm_gray **out);
+void lbm_gray_destroy(lbm_gray *h);
+int lbm_gray_last_error(const lbm_gray *h, char *buf, uint64_t len);
+/* gamma: box_n[0] * box_n[1] * box_n[2] values, x fastest, each in [0, 1] */
+int lbm_gray_set_field(lbm_gray *h, const double *gamma);
+/* back to the initial state (equilibrium at u_in), step counter 0 */
+int lbm_gray_reset(lbm_gray *h);
+/* n steps; forces_out: 6 doubles per step (force, then moment about center) */
+int lbm_gray_run(lbm_gray *h, uint64_t n, double *forces_out);
+/* From the initial state: the objective and its gradient with respect to
+ * every design-box cell's gamma (box order, x fastest).  Leaves the lattice
+ * in the state after spec->steps steps. */
+int lbm_backward(lbm_gray *h, const lbm_adjoint_spec *spec, double *objective, double *dJ_dgamma);
+/* Device time of the last lbm_backward, milliseconds: first forward pass,
+ * recomputed forward segments, reverse sweep. */
+int lbm_gray_backward_times(const lbm_gray *h, double *forward_ms, double *recompute_ms, double *reverse_ms);
+int lbm_gray_stream(lbm_gray *h, void **stream);
+
 /* Allocation-free force and moment sum over wall records (no counterpart in
  * the reference).  For callers that cannot allocate device memory where they
  * need the sum: code running during CUDA graph capture, hosts whose device

@@ -239,3 +239,66 @@ class OracleMulti:
         out = np.zeros(d[0] * d[1] * d[2], dtype=np.uint32)
         self._L.m27_flags(self._h, int(level), out.ctypes.data)
         return out
+
+
+class OracleGray:
+    """The gray-level oracle (forward model and dense-Jacobian adjoint) with
+    the methods of simlab_b200.gray.GrayLattice."""
+
+    def __init__(self, setup, gamma=None, real64: bool = True):
+        L = library()
+        vp, u64 = C.c_void_p, C.c_ulonglong
+        L.gray_create.argtypes = [vp, C.c_int]
+        L.gray_create.restype = vp
+        L.gray_destroy.argtypes = [vp]
+        L.gray_destroy.restype = None
+        L.gray_set_field.argtypes = [vp, vp]
+        L.gray_reset.argtypes = [vp]
+        L.gray_run.argtypes = [vp, u64, vp]
+        L.gray_backward.argtypes = [vp, vp, vp, vp]
+        self._L = L
+        self.setup = setup
+        cs = setup.to_c()
+        h = L.gray_create(C.addressof(cs), int(real64))
+        if not h:
+            buf = C.create_string_buffer(1024)
+            L.orc_last_error(buf, 1024)
+            raise RuntimeError(buf.value.decode())
+        self._h = h
+        if gamma is not None:
+            self.set_field(gamma)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.gray_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_field(self, gamma):
+        g = np.ascontiguousarray(np.asarray(gamma, dtype=np.float64).reshape(-1))
+        assert g.size == self.setup.nbox()
+        self._L.gray_set_field(self._h, g.ctypes.data)
+
+    def reset(self):
+        self._L.gray_reset(self._h)
+
+    def run(self, n: int) -> np.ndarray:
+        out = np.zeros((int(n), 6), dtype=np.float64)
+        self._L.gray_run(self._h, int(n), out.ctypes.data)
+        return out
+
+    def objective(self, spec) -> float:
+        self.reset()
+        return spec.value(self.run(spec.steps))
+
+    def backward(self, spec):
+        J = C.c_double()
+        grad = np.zeros(self.setup.nbox(), dtype=np.float64)
+        cs = spec.to_c()
+        self._L.gray_backward(self._h, C.addressof(cs), C.byref(J), grad.ctypes.data)
+        return J.value, grad

@@ -12,7 +12,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "liboracle.so"
-SOURCES = [HERE / "oracle_capi.cpp", HERE / "d3q19_oracle.hpp", HERE / "d3q27_oracle.hpp", HERE.parent / "include" / "simlab_lbm.h"]
+SOURCES = [HERE / "oracle_capi.cpp", HERE / "d3q19_oracle.hpp", HERE / "d3q27_oracle.hpp", HERE / "gray_oracle.hpp", HERE.parent / "include" / "simlab_lbm.h"]
 
 
 def build_oracle(force: bool = False) -> Path:

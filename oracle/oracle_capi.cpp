@@ -8,6 +8,7 @@
 
 #include "d3q19_oracle.hpp"
 #include "d3q27_oracle.hpp"
+#include "gray_oracle.hpp"
 
 #ifdef _OPENMP
 #include <omp.h>
@@ -33,6 +34,16 @@ struct Multi {
 template <class Fn>
 auto with(void *hp, Fn fn) {
     Multi *h = (Multi *)hp;
+    return h->real64 ? fn(*h->f64) : fn(*h->f32);
+}
+struct GrayH {
+    int real64;
+    oracle::Gray<float> *f32 = nullptr;
+    oracle::Gray<double> *f64 = nullptr;
+};
+template <class Fn>
+auto gwith(void *hp, Fn fn) {
+    GrayH *h = (GrayH *)hp;
     return h->real64 ? fn(*h->f64) : fn(*h->f32);
 }
 }  // namespace
@@ -210,5 +221,47 @@ int m27_flags(void *hp, unsigned level, uint32_t *out) {
 }
 
 unsigned long long m27_fine_steps(void *hp) { return with(hp, [](auto &m) { return (unsigned long long)m.fine_steps; }); }
+
+// ---------------------------------------------------------------- gray level
+void *gray_create(const lbm_gray_setup *st, int real64) {
+    GrayH *h = new GrayH();
+    h->real64 = real64;
+    try {
+        if (real64) { h->f64 = new oracle::Gray<double>(); h->f64->create(*st); }
+        else { h->f32 = new oracle::Gray<float>(); h->f32->create(*st); }
+        return h;
+    } catch (const std::exception &e) {
+        g_err = e.what();
+        delete h->f32;
+        delete h->f64;
+        delete h;
+        return nullptr;
+    }
+}
+
+void gray_destroy(void *hp) {
+    GrayH *h = (GrayH *)hp;
+    if (!h) return;
+    delete h->f32;
+    delete h->f64;
+    delete h;
+}
+
+int gray_set_field(void *hp, const double *gamma) { return gwith(hp, [&](auto &g) { g.set_field(gamma); return 0; }); }
+int gray_reset(void *hp) { return gwith(hp, [&](auto &g) { g.reset(); return 0; }); }
+
+int gray_run(void *hp, unsigned long long n, double *forces) {
+    return gwith(hp, [&](auto &g) {
+        for (unsigned long long k = 0; k < n; k++) {
+            auto f = g.step();
+            if (forces) std::memcpy(forces + 6 * k, f.data(), 6 * sizeof(double));
+        }
+        return 0;
+    });
+}
+
+int gray_backward(void *hp, const lbm_adjoint_spec *sp, double *J, double *grad) {
+    return gwith(hp, [&](auto &g) { *J = g.backward(*sp, grad); return 0; });
+}
 
 }  // extern "C"

@@ -17,7 +17,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libsimlab_lbm.so"
 
-CUDA_SOURCES = ["d3q19_kernels.cu", "lattice.cu", "noalloc.cu", "d3q27_kernels.cu", "mlattice.cu"]
+CUDA_SOURCES = ["d3q19_kernels.cu", "lattice.cu", "noalloc.cu", "d3q27_kernels.cu", "mlattice.cu", "gray.cu"]
 CXX_SOURCES = ["voxel.cpp"]
 HEADERS = ["lbm_device.cuh", "lbm_kernels.h", "voxel.hpp", "d3q27.h"]
 

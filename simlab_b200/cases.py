@@ -13,6 +13,9 @@ smoke check and the bench.
   open outlet and sides; tunnel.rs:764-771) with sponges 16/32/16 cells,
   sponge tau 1.0 and absorbing strength 0.1 (tunnel.rs:206-234, 1006-1007).
   `scale=2` gives the 1024x512x512 arm.
+* `gray_design`: the gray-level adjoint case, 192x96x96 D3Q19 BGK with a
+  64x48x48 design box of smoothed random solid fraction, drag averaged over
+  steps 500-1000, a checkpoint every 50 steps.
 """
 from __future__ import annotations
 
@@ -62,3 +65,53 @@ def arm_reference_area(scale: int = 1) -> float:
 
 # algorithmic bytes per lattice update: 19 populations read and written once plus the u32 flag word
 BYTES_PER_LUP = {Storage.FP32: 156, Storage.FP16: 80, Storage.BF16: 80, Storage.FP64: 308}
+
+
+# ------------------------------------------------------------------ gray-level design case
+def splitmix64(seed: int, n: int) -> np.ndarray:
+    """n uniform doubles in [0, 1) from SplitMix64 (Steele, Lea & Flood 2014),
+    the top 53 bits of each output."""
+    M = (1 << 64) - 1
+    out = np.empty(n, dtype=np.float64)
+    s = seed & M
+    for k in range(n):
+        s = (s + 0x9E3779B97F4A7C15) & M
+        z = s
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & M
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & M
+        z ^= z >> 31
+        out[k] = (z >> 11) * (1.0 / (1 << 53))
+    return out
+
+
+def gaussian_smooth(a: np.ndarray, sigma: float = 3.0, radius: int = 9) -> np.ndarray:
+    """Separable Gaussian filter with mirrored edges (the edge sample repeated)."""
+    x = np.arange(-radius, radius + 1, dtype=np.float64)
+    k = np.exp(-0.5 * (x / sigma) ** 2)
+    k /= k.sum()
+    out = np.asarray(a, dtype=np.float64)
+    for ax in range(out.ndim):
+        pad = [(0, 0)] * out.ndim
+        pad[ax] = (radius, radius)
+        p = np.pad(out, pad, mode="symmetric")
+        out = np.apply_along_axis(lambda r: np.convolve(r, k, mode="valid"), ax, p)
+    return out
+
+
+def gray_design(storage=Storage.FP32, dims=(192, 96, 96), box_lo=(48, 24, 24), box_n=(64, 48, 48), u=0.04, re=100.0, seed=20240601):
+    """The gray-level adjoint case: D3Q19 BGK on 192x96x96, a 64x48x48 design
+    box of solid fraction seeded uniform in [0, 1] (SplitMix64, fixed seed) and
+    smoothed by a Gaussian of sigma 3 cells (radius 9, mirrored edges); inlet
+    u = 0.04, Re = 100 on the box height (nu = u * 48 / 100).  Returns the
+    setup, gamma (box order, x fastest) and the adjoint spec of the mean drag
+    over steps 500-1000 with a checkpoint every 50 steps."""
+    from .gray import AdjointSpec, GraySetup
+
+    nb = int(np.prod(box_n))
+    g = splitmix64(seed, nb).reshape(box_n[2], box_n[1], box_n[0])
+    g = np.clip(gaussian_smooth(g, 3.0, 9), 0.0, 1.0).reshape(-1)
+    nu = u * box_n[1] / re
+    center = [box_lo[k] + 0.5 * (box_n[k] - 1) for k in range(3)]
+    st = GraySetup(dims=list(dims), box_lo=list(box_lo), box_n=list(box_n), nu=nu, u_in=[u, 0.0, 0.0], alpha=1.0, center=center, storage=storage)
+    spec = AdjointSpec(steps=1000, t0=500, t1=1000, checkpoint_every=50, objective=0, dir=[1.0, 0.0, 0.0], recompute=True)
+    return st, g, spec
