@@ -15,6 +15,8 @@ FP32 and BF16 storage and their fraction of the measured HBM copy bandwidth.
 
 With N > 1 (torchrun, one rank per GPU) every rank runs its own replica of
 the case: the step has no data exchange across replicas ("replicas only").
+On one GPU the line also carries the gray-level adjoint's time against one
+forward solve (`adjoint`) and the three-level D3Q27 throughput.
 --impl reference times the reference's update restated on the CPU (the
 oracle; the reference itself is Rust + wgpu/Metal and cannot run here) on
 bounded samples of the same workload.
@@ -212,6 +214,85 @@ def cpu_sample(storage, sample_s: float = 12.0, warm: int = 1):
     return cells / dt / 1e6, cores, f"{cells // (nx * ny * slab)} slabs of {nx}x{ny}x{slab} cells in {dt:.1f} s"
 
 
+def adjoint_ratio():
+    """The gray-level adjoint on its design case (simlab_b200.cases.gray_design:
+    192x96x96 D3Q19 BGK, 64x48x48 design box, drag over steps 500-1000,
+    checkpoint every 50, FP32): device time of one forward solve (1000 steps)
+    and of lbm_backward, with every segment recomputed from its checkpoint and
+    with the trailing moments kept when HBM holds them."""
+    import torch
+
+    from simlab_b200.cases import gray_design
+    from simlab_b200.gray import GrayLattice
+    from simlab_b200.lbm import Storage
+
+    st, gam, spec = gray_design(Storage.FP32)
+    lat = GrayLattice(st, gam)
+    stream = torch.cuda.ExternalStream(lat.stream)
+    lat.run(100)
+    lat.reset()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record()
+    lat.run(spec.steps)
+    with torch.cuda.stream(stream):
+        e1.record()
+    torch.cuda.synchronize()
+    fwd = e0.elapsed_time(e1)
+    out = {"workload": "gray design 192x96x96, box 64x48x48, drag over steps 500-1000, checkpoint every 50, fp32",
+           "forward_ms": round(fwd, 3), "forward_mlups": round(192 * 96 * 96 * spec.steps / fwd / 1e3, 1)}
+    for rc in (True, False):
+        spec.recompute = rc
+        J, g = lat.backward(spec)
+        t = lat.backward_times()
+        tot = t["forward_ms"] + t["recompute_ms"] + t["reverse_ms"]
+        out["recompute_all" if rc else "memory_sized"] = {"backward_ms": round(tot, 3), "ratio": round(tot / fwd, 3),
+                                                           **{k: round(v, 3) for k, v in t.items()}}
+    out["adjoint_over_forward"] = out["recompute_all"]["ratio"]
+    out["objective"] = J
+    lat.close()
+    return out
+
+
+def d3q27_levels():
+    """MLUPS (finest-step definition, tunnel.rs:800-804) of the three-level
+    D3Q27 lattice with the refinement layout of the propeller case (coarse
+    256x128x128, each box 0.63 of its parent per axis), FP32 and FP16."""
+    import torch
+
+    from simlab_b200.lbm import FaceBc, Storage
+    from simlab_b200.mlattice import LevelBox, MultiLattice, MultiSetup
+
+    res = {}
+    for storage in (Storage.FP32, Storage.FP16):
+        F = FaceBc
+        s = MultiSetup(dims0=[256, 128, 128], faces=[F.VELOCITY] + [F.OPEN] * 5, nu0=0.001, u_inf=[0.05, 0, 0], u_init=[0.05, 0, 0],
+                       sponge=[0, 16, 8, 8, 8, 8], sponge_tau=1.0, sponge_sigma=0.1, total_pressure_inlet=True, storage=storage)
+        for l in range(1, 3):
+            d = s.dims(l - 1)
+            n = [int(d[k] * 0.63) for k in range(3)]
+            s.boxes.append(LevelBox(lo=[(d[k] - n[k]) // 2 for k in range(3)], n=n))
+        g = MultiLattice(s)
+        g.advance(16)
+        g.synchronize()
+        stream = torch.cuda.ExternalStream(g.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record()
+        g.advance(64)
+        with torch.cuda.stream(stream):
+            e1.record()
+        g.synchronize()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        cells = g.level_cells()
+        lups = sum(c * 2 ** l for l, c in enumerate(cells)) / 2 ** (len(cells) - 1) * 64
+        res[storage.name.lower()] = round(lups / ms / 1e3, 1)
+        res["cells"] = cells
+        g.close()
+    return res
+
+
 def run_reference(args, ws, rank):
     if rank != 0:
         return
@@ -324,6 +405,9 @@ def main():
         "gpu_launches": 3 * args.steps,
         "kernel_share": {k: round(v / max(kt["faces_ms"] + kt["walls_ms"] + kt["bulk_ms"], 1e-12), 4) for k, v in kt.items() if k != "steps"},
     }
+    if ws == 1:
+        line["adjoint"] = adjoint_ratio()
+        line["d3q27_three_levels_mlups"] = d3q27_levels()
     if rank == 0 and ws == 1 and not args.no_cpu:
         v, cores, sample = cpu_sample(Storage.FP16)
         line["cpu_baseline"] = {"value": round(v, 3), "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
