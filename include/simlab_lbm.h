@@ -98,7 +98,11 @@ typedef struct {
     float q[27];
 } lbm_wall_cell;
 
-/* `Geometry` (lattice.rs:87-92).  kind 0 = None, 1 = Static. */
+/* `Geometry` (lattice.rs:87-92).  kind 0 = None, 1 = Static, 2 = Spin.
+ * Spin: the part's `SpinVoxels` (voxel.rs:492-505, from lbm_voxelize_spin)
+ * and the swept box of lattice cells that holds every cell it can reach;
+ * every box cell becomes a record the GPU re-voxelizes each step from the
+ * step's rotation (StepIn::rot, rot_prev). */
 typedef struct {
     int32_t kind;
     int32_t _pad;
@@ -106,6 +110,16 @@ typedef struct {
     uint64_t nsolid;
     const lbm_wall_cell *walls;/* StaticVoxels::walls */
     uint64_t nwalls;
+    /* kind 2 */
+    const uint32_t *occ_bits;  /* body-frame occupancy, one bit per point of occ_lo + occ_h (i, j, k), x fastest */
+    double occ_lo[3];
+    double occ_h;
+    uint32_t occ_dims[3];
+    uint32_t _pad2;
+    const float *tris;         /* 12 floats per triangle: v0, e1, e2, each padded to 4 (body coordinates) */
+    uint64_t ntri;
+    int32_t box_lo[3];
+    uint32_t box_n[3];
 } lbm_geometry;
 
 /* `SliceDef` (shader.rs:77-84). */
@@ -246,6 +260,27 @@ int lbm_voxelize_static(const double *verts, uint64_t nverts, const uint32_t *tr
 int lbm_voxels_counts(const lbm_voxels *v, uint64_t *nsolid, uint64_t *nwalls);
 int lbm_voxels_copy(const lbm_voxels *v, uint32_t *solid, lbm_wall_cell *walls);
 void lbm_voxels_free(lbm_voxels *v);
+
+/* voxelize_spin (voxel.rs:507-560): body-frame geometry of a spinning part
+ * given in body coordinates (lattice units, origin at the spin centre):
+ * occupancy bits on a grid of spacing h (the reference uses 0.125) and the
+ * surface split into triangles of at most 1.5 cells per edge. */
+typedef struct lbm_spin_voxels lbm_spin_voxels;
+typedef struct {
+    double occ_lo[3];
+    double occ_h;
+    uint32_t occ_dims[3];
+    uint32_t _pad;
+    uint64_t occ_words;        /* u32 words of occupancy bits */
+    uint64_t ntri;
+    double radius;             /* largest distance of the surface from the axis */
+    double axial[2];           /* extent along the axis */
+} lbm_spin_info;
+int lbm_voxelize_spin(const double *verts, uint64_t nverts, const uint32_t *tris, uint64_t ntris, const double axis[3], double h,
+                      lbm_spin_voxels **out);
+int lbm_spin_voxels_info(const lbm_spin_voxels *v, lbm_spin_info *out);
+int lbm_spin_voxels_copy(const lbm_spin_voxels *v, uint32_t *occ_bits, float *tris);
+void lbm_spin_voxels_free(lbm_spin_voxels *v);
 
 /* inside_grid (voxel.rs:73-95): inside test for every point of the grid
  * origin + h * (i, j, k); out: dims[0]*dims[1]*dims[2] bytes (0/1). */

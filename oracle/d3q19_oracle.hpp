@@ -171,6 +171,15 @@ struct D3Q19 {
     std::vector<uint8_t> face_mirror; // free slip: bit a = mirror axis a
     uint64_t steps_done = 0;
     uint32_t seed = 0;  // StepParams.seed of the step being run
+    // spinning part (Geometry::Spin): body-frame occupancy, triangles, swept
+    // box, per-link hit scratch (shader.rs:865-1104)
+    bool moving = false;
+    std::vector<uint32_t> occ;
+    float occ_lo[3] = {0, 0, 0}, occ_invh = 1.f, CENTERF[3] = {0, 0, 0};
+    int32_t occ_n[3] = {0, 0, 0}, box_lo[3] = {0, 0, 0};
+    uint32_t box_n[3] = {0, 0, 0};
+    std::vector<std::array<float, 12>> tris;
+    std::vector<uint32_t> qscr;
 
     // ------------------------------------------------------------ storage
     inline Real L(int d, uint64_t cell) const {
@@ -459,9 +468,46 @@ struct D3Q19 {
                 else { visit(0); if (NX - 1 != 0) visit(NX - 1); }
             }
 
-        // records (lattice.rs:454-482, record_words 202-218)
+        // records (lattice.rs:454-482, record_words 202-218); a spinning part
+        // makes every swept-box cell a record without links (465-480)
         recs.clear();
         std::vector<std::pair<uint32_t, uint32_t>> rec_of;
+        std::vector<lbm_wall_cell> boxwalls;
+        lbm_geometry boxgeom{};
+        for (int k = 0; k < 3; k++) CENTERF[k] = (float)st.center[k];
+        if (geom && geom->kind == 2) {
+            moving = true;
+            for (int k = 0; k < 3; k++) {
+                box_lo[k] = geom->box_lo[k];
+                box_n[k] = geom->box_n[k];
+                occ_lo[k] = (float)geom->occ_lo[k];
+                occ_n[k] = (int32_t)geom->occ_dims[k];
+                if (box_lo[k] < 1 || (int64_t)box_lo[k] + box_n[k] > (int64_t)st.dims[k] - 1)
+                    throw std::runtime_error("the spinning part's swept box leaves the domain");
+            }
+            occ_invh = (float)(1.0 / geom->occ_h);
+            const uint64_t nocc = (uint64_t)occ_n[0] * occ_n[1] * occ_n[2];
+            occ.assign(geom->occ_bits, geom->occ_bits + (nocc + 31) / 32);
+            tris.resize(geom->ntri);
+            for (uint64_t t = 0; t < geom->ntri; t++)
+                for (int j = 0; j < 12; j++) tris[t][j] = geom->tris[12 * t + j];
+            const uint64_t nb = (uint64_t)box_n[0] * box_n[1] * box_n[2];
+            boxwalls.resize(nb);
+            uint64_t k = 0;
+            for (uint32_t z = 0; z < box_n[2]; z++)
+                for (uint32_t y = 0; y < box_n[1]; y++)
+                    for (uint32_t x = 0; x < box_n[0]; x++, k++) {
+                        boxwalls[k].cell = (uint32_t)((((uint64_t)z + box_lo[2]) * NY + y + box_lo[1]) * NX + x + box_lo[0]);
+                        boxwalls[k].mask = 0;
+                        for (int i = 0; i < 27; i++) boxwalls[k].q[i] = 1.0f;
+                    }
+            boxgeom.kind = 1;
+            boxgeom.walls = boxwalls.data();
+            boxgeom.nwalls = nb;
+            geom = &boxgeom;
+            qscr.assign(nb * 27, 0u);
+            for (size_t j = 0; j < qscr.size(); j += 3) qscr[j] = 0x7f7fffffu;
+        }
         if (geom && geom->kind == 1) {
             for (uint64_t r = 0; r < geom->nwalls; r++) {
                 const lbm_wall_cell &w = geom->walls[r];
@@ -638,9 +684,205 @@ struct D3Q19 {
             for (int i = 1; i < 19; i++) rc->fpost[i] = f[i];
             rc->macro[0] = rho;
             for (int a = 0; a < 3; a++) rc->macro[1 + a] = u[a];
+            if (moving)
+                for (int a = 0; a < 3; a++) { Fo[a] = Fo[a] + rc->ft[a]; To[a] = To[a] + rc->ft[3 + a]; }
             for (int a = 0; a < 3; a++) { rc->ft[a] = Fo[a]; rc->ft[3 + a] = To[a]; }
         }
         store_out(n, p, f, false);
+    }
+
+    // ------------------------------------------------------------ spinning part
+    // shader.rs:865-1104 in f32, one rounding per operation (compiled without
+    // contraction), rot row-major with the body axes as columns
+    struct V3f { float x, y, z; };
+    static float dotf(V3f a, V3f b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+    static V3f crossf(V3f a, V3f b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+    static V3f colf(const float *r, int k) { return {r[k], r[3 + k], r[6 + k]}; }
+    static V3f to_body(const float *r, V3f v) { return {dotf(colf(r, 0), v), dotf(colf(r, 1), v), dotf(colf(r, 2), v)}; }
+    static V3f from_body(const float *r, V3f b) {
+        const V3f c0 = colf(r, 0), c1 = colf(r, 1), c2 = colf(r, 2);
+        return {c0.x * b.x + c1.x * b.y + c2.x * b.z, c0.y * b.x + c1.y * b.y + c2.y * b.z, c0.z * b.x + c1.z * b.y + c2.z * b.z};
+    }
+    bool occ_at(V3f b) const {
+        const float gx = std::nearbyint((b.x - occ_lo[0]) * occ_invh), gy = std::nearbyint((b.y - occ_lo[1]) * occ_invh),
+                    gz = std::nearbyint((b.z - occ_lo[2]) * occ_invh);
+        if (!(gx >= 0.f && gy >= 0.f && gz >= 0.f) || gx >= (float)occ_n[0] || gy >= (float)occ_n[1] || gz >= (float)occ_n[2]) return false;
+        const uint64_t l = ((uint64_t)gz * (uint64_t)occ_n[1] + (uint64_t)gy) * (uint64_t)occ_n[0] + (uint64_t)gx;
+        return ((occ[l >> 5] >> (l & 31u)) & 1u) != 0u;
+    }
+    bool solid_at(const float *rot, int x, int y, int z) const {
+        return occ_at(to_body(rot, {(float)x - CENTERF[0], (float)y - CENTERF[1], (float)z - CENTERF[2]}));
+    }
+    static float ray_tri(V3f o, V3f d, V3f v0, V3f e1, V3f e2) {
+        const V3f pv = crossf(d, e2);
+        const float det = dotf(e1, pv);
+        if (std::fabs(det) < 1e-12f) return 9.0f;
+        const float inv = 1.0f / det;
+        const V3f tv = {o.x - v0.x, o.y - v0.y, o.z - v0.z};
+        const float a = dotf(tv, pv) * inv;
+        if (a < 0.0f || a > 1.0f) return 9.0f;
+        const V3f qv = crossf(tv, e1);
+        const float b = dotf(d, qv) * inv;
+        if (b < 0.0f || a + b > 1.0f) return 9.0f;
+        const float t = dotf(e2, qv) * inv;
+        if (t < -1e-4f || t > 1.0f) return 9.0f;
+        return t > 0.0f ? t : 0.0f;  // +0 for -0 too: the hit bits are compared as integers
+    }
+    uint32_t box_index(int x, int y, int z) const {
+        return ((uint32_t)(z - box_lo[2]) * box_n[1] + (uint32_t)(y - box_lo[1])) * box_n[0] + (uint32_t)(x - box_lo[0]);
+    }
+    // shader.rs:902-940
+    void tri_scatter(const float *rot) {
+        for (const auto &tr : tris) {
+            const V3f v0 = from_body(rot, {tr[0], tr[1], tr[2]});
+            const V3f a = {CENTERF[0] + v0.x, CENTERF[1] + v0.y, CENTERF[2] + v0.z};
+            const V3f e1 = from_body(rot, {tr[4], tr[5], tr[6]}), e2 = from_body(rot, {tr[8], tr[9], tr[10]});
+            const V3f nrm = crossf(e1, e2);
+            const float nl = std::sqrt(dotf(nrm, nrm));
+            if (nl < 1e-12f) continue;
+            const V3f nn = {nrm.x / nl, nrm.y / nl, nrm.z / nl};
+            const V3f b = {a.x + e1.x, a.y + e1.y, a.z + e1.z}, c = {a.x + e2.x, a.y + e2.y, a.z + e2.z};
+            const float mn[3] = {std::min(std::min(a.x, b.x), c.x), std::min(std::min(a.y, b.y), c.y), std::min(std::min(a.z, b.z), c.z)};
+            const float mx[3] = {std::max(std::max(a.x, b.x), c.x), std::max(std::max(a.y, b.y), c.y), std::max(std::max(a.z, b.z), c.z)};
+            int lo[3], hi[3];
+            for (int k = 0; k < 3; k++) {
+                lo[k] = std::max((int)std::ceil(mn[k] - 1.415f), box_lo[k]);
+                hi[k] = std::min((int)std::floor(mx[k] + 1.415f), box_lo[k] + (int)box_n[k] - 1);
+            }
+            for (int z = lo[2]; z <= hi[2]; z++)
+                for (int y = lo[1]; y <= hi[1]; y++)
+                    for (int x = lo[0]; x <= hi[0]; x++) {
+                        const V3f pt = {(float)x, (float)y, (float)z};
+                        const float d0 = dotf(nn, {pt.x - a.x, pt.y - a.y, pt.z - a.z});
+                        if (std::fabs(d0) > 1.415f) continue;
+                        const uint32_t k = box_index(x, y, z);
+                        for (int i = 1; i < 19; i += 2) {
+                            const V3f cv = {(float)C19[i][0], (float)C19[i][1], (float)C19[i][2]};
+                            const float d1 = d0 + dotf(nn, cv);
+                            if (d0 * d1 > 0.0f && std::fabs(d0) > 1e-6f) continue;
+                            const float tt = ray_tri(pt, cv, a, e1, e2);
+                            if (tt <= 1.0f) {
+                                const uint64_t o = ((uint64_t)k * 9u + (uint32_t)(i - 1) / 2u) * 3u;
+                                const uint32_t tb = fbits(tt > 0.0f ? tt : 0.0f);
+                                qscr[o] = std::min(qscr[o], tb);
+                                qscr[o + 1] = std::max(qscr[o + 1], tb);
+                                qscr[o + 2] += 1u;
+                            }
+                        }
+                    }
+        }
+    }
+    // shader.rs:953-1104 for every swept-box cell; Q = the previous step's parity
+    void voxelize(const float *rot, const float *rotp, const Real *omega, int Q) {
+        const uint64_t nb = (uint64_t)box_n[0] * box_n[1] * box_n[2];
+        // classification first (reads only the scratch and occupancy), then the
+        // refill (reads neighbours' records of cells that were fluid before,
+        // which nobody writes here)
+#pragma omp parallel for schedule(static)
+        for (long long kk = 0; kk < (long long)nb; kk++) {
+            const uint32_t k = (uint32_t)kk;
+            const int lx = (int)(k % box_n[0]), ly = (int)((k / box_n[0]) % box_n[1]), lz = (int)(k / (box_n[0] * box_n[1]));
+            const int px = lx + box_lo[0], py = ly + box_lo[1], pz = lz + box_lo[2];
+            const uint64_t n = ((uint64_t)pz * NY + py) * NX + px;
+            Rec &rc = recs[k];
+            const Real pc[3] = {(Real)px - CENTER[0], (Real)py - CENTER[1], (Real)pz - CENTER[2]};
+            const bool solid_now = solid_at(rot, px, py, pz), solid_before = solid_at(rotp, px, py, pz);
+            Real Fv[3] = {0, 0, 0};
+            if (solid_now) {
+                flags[n] = 1u | ((k + 1u) << 2);
+                rc.mask = 0;
+                if (!solid_before)
+                    for (int a = 0; a < 3; a++) Fv[a] = rc.macro[0] * rc.macro[1 + a];
+            } else {
+                float qv[19], qx[19];
+                uint32_t nh[19];
+                for (int i = 1; i < 19; i++) {
+                    qv[i] = 9.0f; qx[i] = -1.0f; nh[i] = 0;
+                    if (i & 1) {
+                        const uint64_t o = ((uint64_t)k * 9u + (uint32_t)(i - 1) / 2u) * 3u;
+                        if (qscr[o + 2]) { qv[i] = bitsf(qscr[o]); qx[i] = bitsf(qscr[o + 1]); nh[i] = qscr[o + 2]; }
+                    } else {
+                        const int qx_ = lx + C19[i][0], qy_ = ly + C19[i][1], qz_ = lz + C19[i][2];
+                        if (qx_ >= 0 && qy_ >= 0 && qz_ >= 0 && qx_ < (int)box_n[0] && qy_ < (int)box_n[1] && qz_ < (int)box_n[2]) {
+                            const uint32_t k2 = ((uint32_t)qz_ * box_n[1] + (uint32_t)qy_) * box_n[0] + (uint32_t)qx_;
+                            const uint64_t o = ((uint64_t)k2 * 9u + (uint32_t)(i - 2) / 2u) * 3u;
+                            if (qscr[o + 2]) { qv[i] = 1.0f - bitsf(qscr[o + 1]); qx[i] = 1.0f - bitsf(qscr[o]); nh[i] = qscr[o + 2]; }
+                        }
+                    }
+                }
+                uint32_t mask = 0;
+                for (int i = 1; i < 19; i++) {
+                    if (solid_at(rot, px + C19[i][0], py + C19[i][1], pz + C19[i][2])) {
+                        if (nh[i] == 0) qv[i] = 1.0f;
+                        mask |= 1u << i;
+                    } else if (nh[i] >= 2 && qx[i] - qv[i] > 1e-5f) {
+                        mask |= 1u << i;
+                    } else {
+                        qv[i] = 1.0f;
+                    }
+                }
+                for (int i = 1; i < 19; i++) rc.qh[i - 1] = f32_to_f16(std::min(qv[i], 1.0f));
+                rc.mask = mask;
+            }
+            for (int a = 0; a < 3; a++) { rc.ft[a] = Fv[a]; rc.ft[3 + a] = 0; }
+            if (solid_now) {
+                rc.ft[3] = pc[1] * Fv[2] - pc[2] * Fv[1];
+                rc.ft[4] = pc[2] * Fv[0] - pc[0] * Fv[2];
+                rc.ft[5] = pc[0] * Fv[1] - pc[1] * Fv[0];
+            }
+        }
+        // refill of the cells the part uncovered
+        for (uint32_t k = 0; k < (uint32_t)nb; k++) {
+            const int lx = (int)(k % box_n[0]), ly = (int)((k / box_n[0]) % box_n[1]), lz = (int)(k / (box_n[0] * box_n[1]));
+            const int px = lx + box_lo[0], py = ly + box_lo[1], pz = lz + box_lo[2];
+            const uint64_t n = ((uint64_t)pz * NY + py) * NX + px;
+            if (solid_at(rot, px, py, pz)) continue;
+            Rec &rc = recs[k];
+            const Real pc[3] = {(Real)px - CENTER[0], (Real)py - CENTER[1], (Real)pz - CENTER[2]};
+            Real Fv[3] = {0, 0, 0};
+            if (solid_at(rotp, px, py, pz)) {
+                Real rs = 0, cnt = 0, pis[6] = {0, 0, 0, 0, 0, 0};
+                for (int i = 1; i < 19; i++) {
+                    const int nx_ = px + C19[i][0], ny_ = py + C19[i][1], nz_ = pz + C19[i][2];
+                    if (solid_at(rot, nx_, ny_, nz_) || solid_at(rotp, nx_, ny_, nz_)) continue;
+                    const int qx_ = lx + C19[i][0], qy_ = ly + C19[i][1], qz_ = lz + C19[i][2];
+                    if (!(qx_ >= 0 && qy_ >= 0 && qz_ >= 0 && qx_ < (int)box_n[0] && qy_ < (int)box_n[1] && qz_ < (int)box_n[2])) continue;
+                    const Rec &r2c = recs[((uint32_t)qz_ * box_n[1] + (uint32_t)qy_) * box_n[0] + (uint32_t)qx_];
+                    rs = rs + r2c.macro[0];
+                    cnt = cnt + 1;
+                    F fp;
+                    fp[0] = 0;
+                    for (int j = 1; j < 19; j++) fp[j] = r2c.fpost[j];
+                    const Mom mo2 = moments(fp);
+                    const Real r2 = r2c.macro[0], u2[3] = {r2c.macro[1], r2c.macro[2], r2c.macro[3]};
+                    pis[3] = pis[3] + (mo2.s[3] - r2 * u2[0] * u2[1]);
+                    pis[4] = pis[4] + (mo2.s[4] - r2 * u2[0] * u2[2]);
+                    pis[5] = pis[5] + (mo2.s[5] - r2 * u2[1] * u2[2]);
+                    const Real tr = (mo2.s[0] + mo2.s[1] + mo2.s[2]) / (Real)3;
+                    const Real uu = dot3(u2, u2);
+                    for (int a = 0; a < 3; a++) pis[a] = pis[a] + (mo2.s[a] - tr - r2 * (u2[a] * u2[a] - uu / (Real)3));
+                }
+                const Real rho = cnt > 0 ? rs / cnt : (Real)1;
+                const Real uw[3] = {omega[1] * pc[2] - omega[2] * pc[1], omega[2] * pc[0] - omega[0] * pc[2], omega[0] * pc[1] - omega[1] * pc[0]};
+                F fe = feq(rho - (Real)1, uw);
+                if (cnt > 0) {
+                    for (int j = 0; j < 6; j++) pis[j] = pis[j] / cnt;
+                    const F fq = fneq(pis);
+                    for (int i = 0; i < 19; i++) fe[i] = fe[i] + fq[i];
+                }
+                store_out(n, Q, fe, true);
+                for (int a = 0; a < 3; a++) Fv[a] = -rho * uw[a];
+                for (int i = 1; i < 19; i++) rc.fpost[i] = fe[i];
+                rc.macro[0] = rho;
+                for (int a = 0; a < 3; a++) rc.macro[1 + a] = uw[a];
+            }
+            for (int a = 0; a < 3; a++) rc.ft[a] = Fv[a];
+            rc.ft[3] = pc[1] * Fv[2] - pc[2] * Fv[1];
+            rc.ft[4] = pc[2] * Fv[0] - pc[0] * Fv[2];
+            rc.ft[5] = pc[0] * Fv[1] - pc[1] * Fv[0];
+            flags[n] = (k + 1u) << 2;
+        }
+        for (size_t j = 0; j < qscr.size(); j += 3) { qscr[j] = 0x7f7fffffu; qscr[j + 1] = 0; qscr[j + 2] = 0; }
     }
 
     // one time step (lattice.rs:715-737 for a still geometry); returns the
@@ -649,6 +891,13 @@ struct D3Q19 {
         int p = (int)(steps_done % 2);
         seed = (uint32_t)steps_done * 2654435761u;  // lattice.rs:676
         Real omega[3] = {(Real)sin.omega[0], (Real)sin.omega[1], (Real)sin.omega[2]};
+        if (moving) {
+            float rot[9], rotp[9];
+            for (int r = 0; r < 3; r++)
+                for (int c = 0; c < 3; c++) { rot[3 * r + c] = (float)sin.rot[r][c]; rotp[3 * r + c] = (float)sin.rot_prev[r][c]; }
+            tri_scatter(rot);
+            voxelize(rot, rotp, omega, 1 - p);
+        }
         if (!faces.empty()) faces_step(p);
 #pragma omp parallel for schedule(static)
         for (long long n = 0; n < (long long)N; n++) main_cell((uint64_t)n, p, omega);

@@ -9,6 +9,8 @@ from .lbm import (  # noqa: F401
     LbmError,
     Probes,
     SliceDef,
+    SpinGeometry,
+    SpinVoxels,
     StaticVoxels,
     StepIn,
     Storage,
@@ -16,5 +18,6 @@ from .lbm import (  # noqa: F401
     inside_grid,
     library,
     steps_array,
+    voxelize_spin,
     voxelize_static,
 )

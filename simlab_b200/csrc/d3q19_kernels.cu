@@ -23,6 +23,7 @@
 
 #include "lbm_device.cuh"
 #include "lbm_kernels.h"
+#include "revoxel.cuh"
 
 namespace lbm {
 
@@ -1040,7 +1041,14 @@ template <class S, int P, int COLL>
 static cudaError_t step_t(const LatParams &p, const StepParams &s, cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join,
                           cudaEvent_t *ev) {
     if (ev) cudaEventRecord(ev[0], st);
-    const bool overlap = side && p.nrec && s.nface;
+    if (p.moving) {
+        // re-voxelize the spinning part's swept box for this step's rotation
+        // (lattice.rs:719-723): triangles -> link scratch, cells, scratch reset
+        if (p.ntri) k_tri_scatter<<<blocks_for(p.ntri), BLOCK, 0, st>>>(p, s);
+        k_voxelize<S, 1 - P><<<blocks_for(p.nrec), BLOCK, 0, st>>>(p, s);
+        k_qclear<<<blocks_for((uint64_t)p.nrec * 9u), BLOCK, 0, st>>>(p);
+    }
+    const bool overlap = side && p.nrec && s.nface && !p.moving;
     if (overlap) {
         cudaEventRecord(fork, st);
         cudaStreamWaitEvent(side, fork, 0);

@@ -199,7 +199,10 @@ lbm::StepParams step_params(const lbm_lattice *h, const lbm_step_in &s, uint32_t
         sp.omega_d[a] = s.omega[a];
     }
     for (int r = 0; r < 3; r++)
-        for (int c = 0; c < 3; c++) sp.rot[r * 3 + c] = (float)s.rot[r][c];
+        for (int c = 0; c < 3; c++) {
+            sp.rot[r * 3 + c] = (float)s.rot[r][c];
+            sp.rot_prev[r * 3 + c] = (float)s.rot_prev[r][c];
+        }
     (void)h;
     return sp;
 }
@@ -223,8 +226,7 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     if (st.storage < LBM_STORAGE_FP32 || st.storage > LBM_STORAGE_FP64) throw LbmError(LBM_ERR_INVALID, "unknown storage");
     if (st.collision != LBM_COLLISION_REGULARIZED && st.collision != LBM_COLLISION_BGK) throw LbmError(LBM_ERR_INVALID, "unknown collision");
     if (!(st.nu > 0.0) || !std::isfinite(st.nu)) throw LbmError(LBM_ERR_INVALID, "viscosity must be positive");
-    if (geom && geom->kind != 0 && geom->kind != 1)
-        throw LbmError(LBM_ERR_UNSUPPORTED, "only static geometry is supported by this lattice");
+    if (geom && (geom->kind < 0 || geom->kind > 2)) throw LbmError(LBM_ERR_INVALID, "unknown geometry kind");
     h->setup = st;
 
     // face cells (lattice.rs:283-324) plus free slip: velocity sticks,
@@ -286,6 +288,37 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
         }
     h->nface = (uint32_t)faces.size();
 
+    // A spinning part (lattice.rs:260-271, 465-480): every cell of the swept
+    // box is a record with no cut link and the initial state; the GPU
+    // re-voxelizer rewrites its flag, links and q every step.
+    const lbm_geometry *spin = (geom && geom->kind == 2) ? geom : nullptr;
+    std::vector<lbm_wall_cell> boxwalls;
+    lbm_geometry boxgeom{};
+    if (spin) {
+        for (int k = 0; k < 3; k++)
+            if (spin->box_lo[k] < 1 || (int64_t)spin->box_lo[k] + (int64_t)spin->box_n[k] > (int64_t)st.dims[k] - 1 || spin->box_n[k] == 0)
+                throw LbmError(LBM_ERR_INVALID, "the spinning part's swept box leaves the domain");
+        if (!spin->occ_bits || (spin->ntri && !spin->tris) || !(spin->occ_h > 0.0))
+            throw LbmError(LBM_ERR_INVALID, "spinning part without occupancy grid or triangles");
+        if (spin->ntri >= 0x7fffffffull) throw LbmError(LBM_ERR_INVALID, "too many triangles");
+        const uint64_t nb = (uint64_t)spin->box_n[0] * spin->box_n[1] * spin->box_n[2];
+        if (nb >= 0x3fffffffull) throw LbmError(LBM_ERR_INVALID, "swept box too large");
+        boxwalls.resize(nb);
+        uint64_t k = 0;
+        for (uint32_t z = 0; z < spin->box_n[2]; z++)
+            for (uint32_t y = 0; y < spin->box_n[1]; y++)
+                for (uint32_t x = 0; x < spin->box_n[0]; x++, k++) {
+                    lbm_wall_cell &w = boxwalls[k];
+                    w.cell = (uint32_t)((((uint64_t)z + spin->box_lo[2]) * NY + (uint64_t)y + spin->box_lo[1]) * NX + (uint64_t)x + spin->box_lo[0]);
+                    w.mask = 0;
+                    for (int i = 0; i < 27; i++) w.q[i] = 1.0f;
+                }
+        boxgeom.kind = 1;
+        boxgeom.walls = boxwalls.data();
+        boxgeom.nwalls = nb;
+        geom = &boxgeom;
+    }
+
     // wall records (lattice.rs:454-482; record_words 202-218)
     const bool stat = geom && geom->kind == 1;
     const uint64_t nrec = stat ? geom->nwalls : 0;
@@ -344,7 +377,8 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     const bool tma_ok = (NX * storage_bytes(st.storage)) % 16 == 0 && !per[0] && !per[1];
     std::vector<char> fused(faces.size(), 0);
     uint32_t xinfo[2] = {0, 0};
-    if (tma_ok && !(std::getenv("SIMLAB_LBM_NO_TMA") && std::getenv("SIMLAB_LBM_NO_TMA")[0] == '1')) {
+    // (not with a spinning part, whose re-voxelizer rewrites the box flags)
+    if (tma_ok && !spin && !(std::getenv("SIMLAB_LBM_NO_TMA") && std::getenv("SIMLAB_LBM_NO_TMA")[0] == '1')) {
         for (size_t k = 0; k < faces.size(); k++) {
             const uint64_t c = faces[k], x = c % NX, y = (c / NX) % NY, z = c / (NX * NY);
             if (x != 0 && x != NX - 1) continue;
@@ -455,6 +489,27 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     }
     p.les_on = st.smagorinsky != 0.0;
     p.moving = 0;
+    if (spin) {
+        p.moving = 1;
+        const uint64_t nocc = (uint64_t)spin->occ_dims[0] * spin->occ_dims[1] * spin->occ_dims[2];
+        const uint64_t words_occ = (nocc + 31) / 32;
+        p.occ = (const uint32_t *)h->dalloc(words_occ * 4);
+        ck(cudaMemcpy((void *)p.occ, spin->occ_bits, words_occ * 4, cudaMemcpyHostToDevice), "upload occupancy");
+        for (int k = 0; k < 3; k++) {
+            p.occ_lo[k] = (float)spin->occ_lo[k];
+            p.occ_n[k] = (int32_t)spin->occ_dims[k];
+            p.box_lo[k] = spin->box_lo[k];
+            p.box_n[k] = spin->box_n[k];
+        }
+        p.occ_invh = (float)(1.0 / spin->occ_h);
+        p.ntri = (uint32_t)spin->ntri;
+        p.tris = (const float4 *)h->dalloc(std::max<uint64_t>(spin->ntri, 1) * 48);
+        if (spin->ntri) ck(cudaMemcpy((void *)p.tris, spin->tris, spin->ntri * 48, cudaMemcpyHostToDevice), "upload triangles");
+        std::vector<uint32_t> q0((size_t)nrec * 27, 0u);
+        for (size_t k = 0; k < q0.size(); k += 3) q0[k] = 0x7f7fffffu;  // nearest hit: FLT_MAX
+        p.qscr = (uint32_t *)h->dalloc(q0.size() * 4);
+        ck(cudaMemcpy(p.qscr, q0.data(), q0.size() * 4, cudaMemcpyHostToDevice), "upload link scratch");
+    }
     fill_consts<float>(p.kf, st);
     fill_consts<double>(p.kd, st);
     p.xface_info[0] = xinfo[0];
@@ -482,7 +537,7 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     // the wall kernel may overlap the face kernel when no wall cell is within
     // three cells of a non-periodic boundary (its slots then never meet the
     // faces' slots or the inner cells the faces read)
-    bool walls_far = nrec > 0 && !faces.empty();
+    bool walls_far = nrec > 0 && !faces.empty() && !spin;
     for (uint64_t r = 0; walls_far && r < nrec; r++) {
         const uint64_t c = geom->walls[r].cell;
         const uint64_t q[3] = {c % NX, (c / NX) % NY, c / (NX * NY)};
@@ -855,6 +910,52 @@ int lbm_voxels_copy(const lbm_voxels *v, uint32_t *solid, lbm_wall_cell *walls) 
 }
 
 void lbm_voxels_free(lbm_voxels *v) { delete v; }
+
+struct lbm_spin_voxels {
+    lbm::SpinVoxels v;
+};
+
+int lbm_voxelize_spin(const double *verts, uint64_t nverts, const uint32_t *tris, uint64_t ntris, const double axis[3], double h,
+                      lbm_spin_voxels **out) {
+    if (!out || !axis || (nverts && !verts) || (ntris && !tris)) { g_error = "null argument"; return LBM_ERR_INVALID; }
+    if (!(h > 0.0)) { g_error = "grid spacing must be positive"; return LBM_ERR_INVALID; }
+    return guard(nullptr, [&] {
+        lbm::Surface s;
+        s.verts.resize(nverts);
+        for (uint64_t k = 0; k < nverts; k++) s.verts[k] = {verts[3 * k], verts[3 * k + 1], verts[3 * k + 2]};
+        s.tris.resize(ntris);
+        for (uint64_t k = 0; k < ntris; k++) {
+            for (int j = 0; j < 3; j++)
+                if (tris[3 * k + j] >= nverts) throw LbmError(LBM_ERR_INVALID, "triangle index out of range");
+            s.tris[k] = {tris[3 * k], tris[3 * k + 1], tris[3 * k + 2]};
+        }
+        lbm_spin_voxels *v = new lbm_spin_voxels();
+        v->v = lbm::voxelize_spin(s, {axis[0], axis[1], axis[2]}, h);
+        *out = v;
+    });
+}
+
+int lbm_spin_voxels_info(const lbm_spin_voxels *v, lbm_spin_info *out) {
+    if (!v || !out) return LBM_ERR_INVALID;
+    std::memset(out, 0, sizeof(*out));
+    for (int k = 0; k < 3; k++) { out->occ_lo[k] = v->v.occ_lo[k]; out->occ_dims[k] = (uint32_t)v->v.occ_dims[k]; }
+    out->occ_h = v->v.occ_h;
+    out->occ_words = v->v.occ_bits.size();
+    out->ntri = v->v.tris.size();
+    out->radius = v->v.radius;
+    out->axial[0] = v->v.axial[0];
+    out->axial[1] = v->v.axial[1];
+    return LBM_OK;
+}
+
+int lbm_spin_voxels_copy(const lbm_spin_voxels *v, uint32_t *occ_bits, float *tris) {
+    if (!v || !occ_bits || (!tris && !v->v.tris.empty())) return LBM_ERR_INVALID;
+    std::memcpy(occ_bits, v->v.occ_bits.data(), v->v.occ_bits.size() * 4);
+    for (size_t k = 0; k < v->v.tris.size(); k++) std::memcpy(tris + 12 * k, v->v.tris[k].data(), 48);
+    return LBM_OK;
+}
+
+void lbm_spin_voxels_free(lbm_spin_voxels *v) { delete v; }
 
 int lbm_inside_grid(const double *verts, uint64_t nverts, const uint32_t *tris, uint64_t ntris, const double origin[3], double h,
                     const uint32_t dims[3], uint8_t *out) {

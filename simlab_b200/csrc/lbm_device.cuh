@@ -113,6 +113,17 @@ struct LatParams {
     const double *sp_tabd;     // the same in FP64
     uint32_t xface_info[2];    // face info (kind | mirror << 2) of the -x and +x faces, for fused x faces
     int tma;                   // the staged bulk kernel applies (NX * element size % 16 == 0)
+    // spinning part (Geometry::Spin, lattice.rs:87-92): every cell of the swept
+    // box is a record, re-voxelized each step from the rotated surface
+    const uint32_t *occ;       // body-frame occupancy bits on a fine grid
+    float occ_lo[3];
+    float occ_invh;
+    int32_t occ_n[3];
+    const float4 *tris;        // 3 per triangle: v0, e1, e2 (body frame)
+    uint32_t ntri;
+    int32_t box_lo[3];
+    uint32_t box_n[3];
+    uint32_t *qscr;            // 9 links x (nearest t, farthest t, hits) per box cell
     Consts<float> kf;
     Consts<double> kd;
 };
@@ -126,6 +137,7 @@ struct StepParams {
     float omega[3];  // angular velocity, rad per step
     double omega_d[3];
     float rot[9];    // body axes in lattice coordinates, row-major (columns = axes)
+    float rot_prev[9];  // the same for the previous step
 };
 
 template <class R> __device__ __forceinline__ const Consts<R> &K(const LatParams &p);

@@ -383,3 +383,79 @@ StaticVoxels voxelize_static(const Surface &s, std::array<size_t, 3> dims, int l
 }
 
 }  // namespace lbm
+
+namespace lbm {
+
+// voxel.rs:562-584: splits triangles at their edge midpoints (1 into 4) until
+// no edge is longer than max_edge
+Surface subdivide(const Surface &s, double max_edge) {
+    Surface o;
+    o.verts = s.verts;
+    std::vector<std::array<uint32_t, 3>> stack(s.tris.begin(), s.tris.end());
+    auto len = [](const std::array<double, 3> &a, const std::array<double, 3> &b) {
+        return std::sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
+    };
+    while (!stack.empty()) {
+        const std::array<uint32_t, 3> t = stack.back();
+        stack.pop_back();
+        const auto a = o.verts[t[0]], b = o.verts[t[1]], c = o.verts[t[2]];
+        if (std::max(std::max(len(a, b), len(b, c)), len(c, a)) <= max_edge || o.tris.size() > 50000000u) {
+            o.tris.push_back(t);
+            continue;
+        }
+        auto mid = [&](const std::array<double, 3> &p, const std::array<double, 3> &q) {
+            o.verts.push_back({(p[0] + q[0]) / 2.0, (p[1] + q[1]) / 2.0, (p[2] + q[2]) / 2.0});
+            return (uint32_t)(o.verts.size() - 1);
+        };
+        const uint32_t ab = mid(a, b), bc = mid(b, c), ca = mid(c, a);
+        stack.push_back({t[0], ab, ca});
+        stack.push_back({ab, t[1], bc});
+        stack.push_back({ca, bc, t[2]});
+        stack.push_back({ab, bc, ca});
+    }
+    return o;
+}
+
+// voxel.rs:507-560: occupancy on a grid of spacing h around the part (a margin
+// of 2h), triangles as (v0, e1, e2) in f32, radius and axial extent
+SpinVoxels voxelize_spin(const Surface &s, std::array<double, 3> axis, double h) {
+    SpinVoxels v;
+    if (s.verts.empty()) throw std::runtime_error("empty surface");
+    std::array<double, 3> lo = s.verts[0], hi = s.verts[0];
+    for (const auto &p : s.verts)
+        for (int k = 0; k < 3; k++) { lo[k] = std::min(lo[k], p[k]); hi[k] = std::max(hi[k], p[k]); }
+    const double m = 2.0 * h;
+    GridSpec g;
+    for (int k = 0; k < 3; k++) {
+        v.occ_lo[k] = lo[k] - m;
+        v.occ_dims[k] = (size_t)std::ceil((hi[k] - lo[k] + 2.0 * m) / h) + 1;
+    }
+    g.origin = v.occ_lo;
+    g.h = h;
+    g.dims = v.occ_dims;
+    v.occ_h = h;
+    const std::vector<uint8_t> inside = inside_grid(s, g);
+    v.occ_bits.assign((inside.size() + 31) / 32, 0u);
+    for (size_t l = 0; l < inside.size(); l++)
+        if (inside[l]) v.occ_bits[l >> 5] |= 1u << (l & 31);
+    const Surface fine = subdivide(s, 1.5);
+    v.tris.reserve(fine.tris.size());
+    for (const auto &t : fine.tris) {
+        const auto a = fine.verts[t[0]], b = fine.verts[t[1]], c = fine.verts[t[2]];
+        v.tris.push_back({(float)a[0], (float)a[1], (float)a[2], 0.f, (float)(b[0] - a[0]), (float)(b[1] - a[1]), (float)(b[2] - a[2]), 0.f,
+                          (float)(c[0] - a[0]), (float)(c[1] - a[1]), (float)(c[2] - a[2]), 0.f});
+    }
+    double amin = std::numeric_limits<double>::infinity(), amax = -amin;
+    for (const auto &p : s.verts) {
+        const double a = p[0] * axis[0] + p[1] * axis[1] + p[2] * axis[2];
+        const double r2 = std::max(p[0] * p[0] + p[1] * p[1] + p[2] * p[2] - a * a, 0.0);
+        v.radius = std::max(v.radius, std::sqrt(r2));
+        amin = std::min(amin, a);
+        amax = std::max(amax, a);
+    }
+    v.axial[0] = amin;
+    v.axial[1] = amax;
+    return v;
+}
+
+}  // namespace lbm

@@ -30,7 +30,19 @@ struct StaticVoxels {  // voxel.rs:337-344
     std::array<size_t, 3> lo{}, hi{};
 };
 
+struct SpinVoxels {  // voxel.rs:492-505 (the diagnostic bins are left out)
+    std::array<double, 3> occ_lo{};
+    double occ_h = 0.125;
+    std::array<size_t, 3> occ_dims{};
+    std::vector<uint32_t> occ_bits;
+    std::vector<std::array<float, 12>> tris;  // v0, e1, e2 (body frame), each padded to 4
+    double radius = 0;
+    double axial[2] = {0, 0};
+};
+
 std::vector<uint8_t> inside_grid(const Surface &s, const GridSpec &g);
+Surface subdivide(const Surface &s, double max_edge);
+SpinVoxels voxelize_spin(const Surface &s, std::array<double, 3> axis, double h);
 bool seg_tri(const double o[3], const double d[3], const double t0[3], const double t1[3], const double t2[3], double *t);
 StaticVoxels voxelize_static(const Surface &s, std::array<size_t, 3> dims, int lattice);
 

@@ -94,6 +94,28 @@ class _Geometry(C.Structure):
         ("nsolid", C.c_uint64),
         ("walls", C.c_void_p),
         ("nwalls", C.c_uint64),
+        ("occ_bits", C.POINTER(C.c_uint32)),
+        ("occ_lo", C.c_double * 3),
+        ("occ_h", C.c_double),
+        ("occ_dims", C.c_uint32 * 3),
+        ("_pad2", C.c_uint32),
+        ("tris", C.POINTER(C.c_float)),
+        ("ntri", C.c_uint64),
+        ("box_lo", C.c_int32 * 3),
+        ("box_n", C.c_uint32 * 3),
+    ]
+
+
+class _SpinInfo(C.Structure):
+    _fields_ = [
+        ("occ_lo", C.c_double * 3),
+        ("occ_h", C.c_double),
+        ("occ_dims", C.c_uint32 * 3),
+        ("_pad", C.c_uint32),
+        ("occ_words", C.c_uint64),
+        ("ntri", C.c_uint64),
+        ("radius", C.c_double),
+        ("axial", C.c_double * 2),
     ]
 
 
@@ -175,6 +197,11 @@ def library() -> C.CDLL:
     L.lbm_voxels_free.argtypes = [vp]
     L.lbm_voxels_free.restype = None
     L.lbm_inside_grid.argtypes = [dp, u64, C.POINTER(C.c_uint32), u64, dp, C.c_double, C.POINTER(C.c_uint32), C.POINTER(C.c_uint8)]
+    L.lbm_voxelize_spin.argtypes = [dp, u64, C.POINTER(C.c_uint32), u64, dp, C.c_double, C.POINTER(vp)]
+    L.lbm_spin_voxels_info.argtypes = [vp, C.POINTER(_SpinInfo)]
+    L.lbm_spin_voxels_copy.argtypes = [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_float)]
+    L.lbm_spin_voxels_free.argtypes = [vp]
+    L.lbm_spin_voxels_free.restype = None
     L.lbm_record_forces_noalloc.argtypes = [vp, u64, vp, vp]
     L.lbm_record_forces_noalloc_max.restype = u64
     L.lbm_noalloc_error.argtypes = [C.c_char_p, u64]
@@ -259,6 +286,30 @@ class StaticVoxels:
 
 
 @dataclass
+class SpinVoxels:
+    """`SpinVoxels` (voxel.rs:492-505): body-frame occupancy bits on a grid of
+    spacing occ_h from occ_lo, and the surface as (v0, e1, e2) triangles."""
+
+    occ_lo: tuple
+    occ_h: float
+    occ_dims: tuple
+    occ_bits: np.ndarray  # uint32
+    tris: np.ndarray      # float32, (ntri, 12)
+    radius: float
+    axial: tuple
+
+
+@dataclass
+class SpinGeometry:
+    """`Geometry::Spin` (lattice.rs:87-92): the part and the swept box of
+    lattice cells that holds every cell it can reach."""
+
+    vox: SpinVoxels
+    box_lo: Sequence[int]
+    box_n: Sequence[int]
+
+
+@dataclass
 class SliceDef:
     """`SliceDef` (shader.rs:77-84)."""
 
@@ -313,11 +364,27 @@ def steps_array(steps: Iterable[StepIn] | int, sample: bool = False) -> np.ndarr
     return a
 
 
-def geometry_struct(geom: StaticVoxels | None) -> tuple[_Geometry, list]:
+def geometry_struct(geom) -> tuple[_Geometry, list]:
+    """The C struct of None, a StaticVoxels or a SpinGeometry."""
     g = _Geometry()
     keep: list = []
     if geom is None:
         g.kind = 0
+        return g, keep
+    if isinstance(geom, SpinGeometry):
+        v = geom.vox
+        occ = np.ascontiguousarray(v.occ_bits, dtype=np.uint32)
+        tris = np.ascontiguousarray(v.tris, dtype=np.float32).reshape(-1, 12)
+        keep += [occ, tris]
+        g.kind = 2
+        g.occ_bits = occ.ctypes.data_as(C.POINTER(C.c_uint32))
+        g.occ_lo[:] = [float(x) for x in v.occ_lo]
+        g.occ_h = float(v.occ_h)
+        g.occ_dims[:] = [int(x) for x in v.occ_dims]
+        g.tris = tris.ctypes.data_as(C.POINTER(C.c_float))
+        g.ntri = len(tris)
+        g.box_lo[:] = [int(x) for x in geom.box_lo]
+        g.box_n[:] = [int(x) for x in geom.box_n]
         return g, keep
     solid = np.ascontiguousarray(geom.solid, dtype=np.uint32)
     walls = np.ascontiguousarray(geom.walls)
@@ -539,6 +606,29 @@ def voxelize_static(verts, tris, dims: Sequence[int], lattice: int = 19) -> Stat
     finally:
         L.lbm_voxels_free(h)
     return StaticVoxels(solid=solid, walls=walls)
+
+
+def voxelize_spin(verts, tris, axis: Sequence[float] = (0.0, 0.0, 1.0), h: float = 0.125) -> SpinVoxels:
+    """voxelize_spin (voxel.rs:507-560): the part in body coordinates (lattice
+    units, origin at the spin centre)."""
+    L = library()
+    v, t = _surface_arrays(verts, tris)
+    ax = (C.c_double * 3)(*[float(x) for x in axis])
+    hnd = C.c_void_p()
+    rc = L.lbm_voxelize_spin(v.ctypes.data_as(C.POINTER(C.c_double)), len(v), t.ctypes.data_as(C.POINTER(C.c_uint32)), len(t), ax, float(h),
+                             C.byref(hnd))
+    if rc != 0:
+        raise _global_error(rc)
+    try:
+        info = _SpinInfo()
+        L.lbm_spin_voxels_info(hnd, C.byref(info))
+        occ = np.zeros(int(info.occ_words), dtype=np.uint32)
+        tr = np.zeros((int(info.ntri), 12), dtype=np.float32)
+        L.lbm_spin_voxels_copy(hnd, occ.ctypes.data_as(C.POINTER(C.c_uint32)), tr.ctypes.data_as(C.POINTER(C.c_float)))
+    finally:
+        L.lbm_spin_voxels_free(hnd)
+    return SpinVoxels(occ_lo=tuple(info.occ_lo), occ_h=info.occ_h, occ_dims=tuple(info.occ_dims), occ_bits=occ, tris=tr, radius=info.radius,
+                      axial=tuple(info.axial))
 
 
 def inside_grid(verts, tris, origin: Sequence[float], h: float, dims: Sequence[int]) -> np.ndarray:
