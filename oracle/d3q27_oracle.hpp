@@ -95,7 +95,18 @@ struct Multi27 {
         uint32_t src = 0, mw = 0, mold = 0, mnew = 0, seed = 0;
         Real blend = 0;
         Real omega[3] = {0, 0, 0};
+        float rot[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, rot_prev[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
     };
+    // spinning part on the finest level (no reference counterpart): the D3Q19
+    // re-voxelizer of shader.rs:865-1104 carried to 27 directions, links kept
+    // at the cell they leave along i = 14..26
+    bool moving = false;
+    std::vector<uint32_t> occ;
+    float occ_lo[3] = {0, 0, 0}, occ_invh = 1.f, CENTERF[3] = {0, 0, 0};
+    int32_t occ_n[3] = {0, 0, 0}, box_lo[3] = {0, 0, 0};
+    uint32_t box_n[3] = {0, 0, 0};
+    std::vector<std::array<float, 12>> tris;
+    std::vector<uint32_t> qscr;
 
     int storage = LBM_STORAGE_FP32;
     bool ABS_U = false, TOTAL_P = false;
@@ -346,9 +357,47 @@ struct Multi27 {
             scale[l] = scale[l - 1] / 2.0;
             for (int k = 0; k < 3; k++) org[l][k] = org[l - 1][k] + s.boxes[l - 1].lo[k] * scale[l - 1];
         }
-        // records (mlattice.rs:178-192, 345-354)
+        // records (mlattice.rs:178-192, 345-354); a spinning part makes every
+        // swept-box cell of the finest level a record without links
         std::vector<std::pair<uint32_t, uint32_t>> rec_of;
         std::vector<uint32_t> solid;
+        std::vector<lbm_wall_cell> boxwalls;
+        lbm_geometry boxgeom{};
+        for (int k = 0; k < 3; k++) CENTERF[k] = (float)s.center[k];
+        if (geom && geom->kind == 2) {
+            const auto fd = dims(finest);
+            moving = true;
+            for (int k = 0; k < 3; k++) {
+                box_lo[k] = geom->box_lo[k];
+                box_n[k] = geom->box_n[k];
+                occ_lo[k] = (float)geom->occ_lo[k];
+                occ_n[k] = (int32_t)geom->occ_dims[k];
+                if (box_lo[k] < 1 || (int64_t)box_lo[k] + box_n[k] > (int64_t)fd[k] - 1)
+                    throw std::runtime_error("the spinning part's swept box leaves the finest level");
+            }
+            occ_invh = (float)(1.0 / geom->occ_h);
+            const uint64_t nocc = (uint64_t)occ_n[0] * occ_n[1] * occ_n[2];
+            occ.assign(geom->occ_bits, geom->occ_bits + (nocc + 31) / 32);
+            tris.resize(geom->ntri);
+            for (uint64_t t = 0; t < geom->ntri; t++)
+                for (int j = 0; j < 12; j++) tris[t][j] = geom->tris[12 * t + j];
+            const uint64_t nb = (uint64_t)box_n[0] * box_n[1] * box_n[2];
+            boxwalls.resize(nb);
+            uint64_t k = 0;
+            for (uint32_t z = 0; z < box_n[2]; z++)
+                for (uint32_t y = 0; y < box_n[1]; y++)
+                    for (uint32_t x = 0; x < box_n[0]; x++, k++) {
+                        boxwalls[k].cell = (uint32_t)((((uint64_t)z + box_lo[2]) * fd[1] + y + box_lo[1]) * fd[0] + x + box_lo[0]);
+                        boxwalls[k].mask = 0;
+                        for (int i = 0; i < 27; i++) boxwalls[k].q[i] = 1.0f;
+                    }
+            boxgeom.kind = 1;
+            boxgeom.walls = boxwalls.data();
+            boxgeom.nwalls = nb;
+            geom = &boxgeom;
+            qscr.assign(nb * 39, 0u);
+            for (size_t j = 0; j < qscr.size(); j += 3) qscr[j] = 0x7f7fffffu;
+        }
         if (geom && geom->kind == 1) {
             nrec = (uint32_t)geom->nwalls;
             rec_words.assign((size_t)nrec * q27::RS, 0u);
@@ -602,6 +651,8 @@ struct Multi27 {
             }
             if (rec != 0) {
                 const uint32_t r = rec - 1;
+                if (moving)
+                    for (int k = 0; k < 3; k++) { Fv[k] += rec_ft[(size_t)r * 6 + k]; Tv[k] += rec_ft[(size_t)r * 6 + 3 + k]; }
                 for (int k = 0; k < 3; k++) { rec_ft[(size_t)r * 6 + k] = Fv[k]; rec_ft[(size_t)r * 6 + 3 + k] = Tv[k]; }
                 for (int k = 0; k < 6; k++) rec_words[(size_t)r * q27::RS + q27::R_FT + k] = fbits((float)rec_ft[(size_t)r * 6 + k]);
             }
@@ -681,6 +732,170 @@ struct Multi27 {
         }
     }
 
+    // ------------------------------------------------------------ spinning part
+    // f32 geometry, one rounding per operation (compiled without contraction)
+    struct V3f { float x, y, z; };
+    static float dotf(V3f a, V3f b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+    static V3f crossf(V3f a, V3f b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+    static V3f colf(const float *r, int k) { return {r[k], r[3 + k], r[6 + k]}; }
+    static V3f to_body(const float *r, V3f v) { return {dotf(colf(r, 0), v), dotf(colf(r, 1), v), dotf(colf(r, 2), v)}; }
+    static V3f from_body(const float *r, V3f b) {
+        const V3f c0 = colf(r, 0), c1 = colf(r, 1), c2 = colf(r, 2);
+        return {c0.x * b.x + c1.x * b.y + c2.x * b.z, c0.y * b.x + c1.y * b.y + c2.y * b.z, c0.z * b.x + c1.z * b.y + c2.z * b.z};
+    }
+    bool solid_at(const float *rot, int x, int y, int z) const {
+        const V3f b = to_body(rot, {(float)x - CENTERF[0], (float)y - CENTERF[1], (float)z - CENTERF[2]});
+        const float gx = std::nearbyint((b.x - occ_lo[0]) * occ_invh), gy = std::nearbyint((b.y - occ_lo[1]) * occ_invh),
+                    gz = std::nearbyint((b.z - occ_lo[2]) * occ_invh);
+        if (!(gx >= 0.f && gy >= 0.f && gz >= 0.f) || gx >= (float)occ_n[0] || gy >= (float)occ_n[1] || gz >= (float)occ_n[2]) return false;
+        const uint64_t li = ((uint64_t)gz * (uint64_t)occ_n[1] + (uint64_t)gy) * (uint64_t)occ_n[0] + (uint64_t)gx;
+        return ((occ[li >> 5] >> (li & 31u)) & 1u) != 0u;
+    }
+    static float ray_tri(V3f o, V3f d, V3f v0, V3f e1, V3f e2) {
+        const V3f pv = crossf(d, e2);
+        const float det = dotf(e1, pv);
+        if (std::fabs(det) < 1e-12f) return 9.0f;
+        const float inv = 1.0f / det;
+        const V3f tv = {o.x - v0.x, o.y - v0.y, o.z - v0.z};
+        const float a = dotf(tv, pv) * inv;
+        if (a < 0.0f || a > 1.0f) return 9.0f;
+        const V3f qv = crossf(tv, e1);
+        const float b = dotf(d, qv) * inv;
+        if (b < 0.0f || a + b > 1.0f) return 9.0f;
+        const float t = dotf(e2, qv) * inv;
+        if (t < -1e-4f || t > 1.0f) return 9.0f;
+        return t > 0.0f ? t : 0.0f;
+    }
+    bool in_box(int lx, int ly, int lz) const {
+        return lx >= 0 && ly >= 0 && lz >= 0 && lx < (int)box_n[0] && ly < (int)box_n[1] && lz < (int)box_n[2];
+    }
+    void revoxel(Level &l, const Par &st) {
+        // links: triangles rotated to this step's angle against the links around them
+        const float REACH = 1.733f;
+        for (const auto &tr : tris) {
+            const V3f v0 = from_body(st.rot, {tr[0], tr[1], tr[2]});
+            const V3f a = {CENTERF[0] + v0.x, CENTERF[1] + v0.y, CENTERF[2] + v0.z};
+            const V3f e1 = from_body(st.rot, {tr[4], tr[5], tr[6]}), e2 = from_body(st.rot, {tr[8], tr[9], tr[10]});
+            const V3f nrm = crossf(e1, e2);
+            const float nl = std::sqrt(dotf(nrm, nrm));
+            if (nl < 1e-12f) continue;
+            const V3f nn = {nrm.x / nl, nrm.y / nl, nrm.z / nl};
+            const V3f b = {a.x + e1.x, a.y + e1.y, a.z + e1.z}, c = {a.x + e2.x, a.y + e2.y, a.z + e2.z};
+            const float mn[3] = {std::min(std::min(a.x, b.x), c.x), std::min(std::min(a.y, b.y), c.y), std::min(std::min(a.z, b.z), c.z)};
+            const float mx[3] = {std::max(std::max(a.x, b.x), c.x), std::max(std::max(a.y, b.y), c.y), std::max(std::max(a.z, b.z), c.z)};
+            int lo[3], hi[3];
+            for (int k = 0; k < 3; k++) {
+                lo[k] = std::max((int)std::ceil(mn[k] - REACH), box_lo[k]);
+                hi[k] = std::min((int)std::floor(mx[k] + REACH), box_lo[k] + (int)box_n[k] - 1);
+            }
+            for (int z = lo[2]; z <= hi[2]; z++)
+                for (int y = lo[1]; y <= hi[1]; y++)
+                    for (int x = lo[0]; x <= hi[0]; x++) {
+                        const V3f pt = {(float)x, (float)y, (float)z};
+                        const float d0 = dotf(nn, {pt.x - a.x, pt.y - a.y, pt.z - a.z});
+                        if (std::fabs(d0) > REACH) continue;
+                        const uint32_t k = ((uint32_t)(z - box_lo[2]) * box_n[1] + (uint32_t)(y - box_lo[1])) * box_n[0] + (uint32_t)(x - box_lo[0]);
+                        for (int i = 14; i < 27; i++) {
+                            const V3f cv = {(float)q27::cx(i), (float)q27::cy(i), (float)q27::cz(i)};
+                            const float d1 = d0 + dotf(nn, cv);
+                            if (d0 * d1 > 0.0f && std::fabs(d0) > 1e-6f) continue;
+                            const float tt = ray_tri(pt, cv, a, e1, e2);
+                            if (tt <= 1.0f) {
+                                const uint64_t o = ((uint64_t)k * 13u + (uint32_t)(i - 14)) * 3u;
+                                const uint32_t tb = fbits(tt > 0.0f ? tt : 0.0f);
+                                qscr[o] = std::min(qscr[o], tb);
+                                qscr[o + 1] = std::max(qscr[o + 1], tb);
+                                qscr[o + 2] += 1u;
+                            }
+                        }
+                    }
+        }
+        // cells: solid or fluid, links and q, refill, cover / uncover momentum
+        for (uint32_t k = 0; k < nrec; k++) {
+            const int lx = (int)(k % box_n[0]), ly = (int)((k / box_n[0]) % box_n[1]), lz = (int)(k / (box_n[0] * box_n[1]));
+            const int px = lx + box_lo[0], py = ly + box_lo[1], pz = lz + box_lo[2];
+            const uint64_t n = cidx(l, (uint32_t)px, (uint32_t)py, (uint32_t)pz);
+            uint32_t *w = &rec_words[(size_t)k * q27::RS];
+            const Real pc[3] = {(Real)px - l.CENTER[0], (Real)py - l.CENTER[1], (Real)pz - l.CENTER[2]};
+            const bool solid_now = solid_at(st.rot, px, py, pz), solid_before = solid_at(st.rot_prev, px, py, pz);
+            Real Fv[3] = {0, 0, 0};
+            if (solid_now) {
+                l.flags[n] = q27::T_SOLID | ((k + 1u) << 3);
+                w[q27::R_MASK] = 0;
+                if (!solid_before) {
+                    const Mom mo = moments(own(l, st.src, n));
+                    for (int c = 0; c < 3; c++) Fv[c] = mo.j[c];
+                }
+            } else {
+                float qv[27], qx[27];
+                uint32_t nh[27];
+                for (int i = 0; i < 27; i++) {
+                    qv[i] = 9.0f; qx[i] = -1.0f; nh[i] = 0;
+                    if (i == q27::REST) continue;
+                    if (i > q27::REST) {
+                        const uint64_t o = ((uint64_t)k * 13u + (uint32_t)(i - 14)) * 3u;
+                        if (qscr[o + 2]) { qv[i] = bitsf(qscr[o]); qx[i] = bitsf(qscr[o + 1]); nh[i] = qscr[o + 2]; }
+                    } else if (in_box(lx + q27::cx(i), ly + q27::cy(i), lz + q27::cz(i))) {
+                        const uint32_t k2 = ((uint32_t)(lz + q27::cz(i)) * box_n[1] + (uint32_t)(ly + q27::cy(i))) * box_n[0] + (uint32_t)(lx + q27::cx(i));
+                        const uint64_t o = ((uint64_t)k2 * 13u + (uint32_t)(26 - i - 14)) * 3u;
+                        if (qscr[o + 2]) { qv[i] = 1.0f - bitsf(qscr[o + 1]); qx[i] = 1.0f - bitsf(qscr[o]); nh[i] = qscr[o + 2]; }
+                    }
+                }
+                uint32_t mask = 0;
+                for (int i = 0; i < 27; i++) {
+                    if (i == q27::REST) continue;
+                    if (solid_at(st.rot, px + q27::cx(i), py + q27::cy(i), pz + q27::cz(i))) {
+                        if (nh[i] == 0) qv[i] = 1.0f;
+                        mask |= 1u << i;
+                    } else if (nh[i] >= 2 && qx[i] - qv[i] > 1e-5f) {
+                        mask |= 1u << i;
+                    } else {
+                        qv[i] = 1.0f;
+                    }
+                }
+                for (int wd = 0; wd < 13; wd++) {
+                    const int i0 = 2 * wd < 13 ? 2 * wd : 2 * wd + 1, i1 = 2 * wd + 1 < 13 ? 2 * wd + 1 : 2 * wd + 2;
+                    const uint16_t lo = f32_to_f16(std::min(qv[i0], 1.0f)), hi = f32_to_f16(std::min(qv[i1], 1.0f));
+                    w[q27::R_Q + wd] = (uint32_t)lo | ((uint32_t)hi << 16);
+                    rec_q[(size_t)k * 26 + 2 * wd] = (Real)f16_to_f32(lo);
+                    rec_q[(size_t)k * 26 + 2 * wd + 1] = (Real)f16_to_f32(hi);
+                }
+                w[q27::R_MASK] = mask;
+                if (solid_before) {
+                    Real rs = 0, cnt = 0, pis[6] = {0, 0, 0, 0, 0, 0};
+                    for (int i = 0; i < 27; i++) {
+                        if (i == q27::REST) continue;
+                        const int x2 = px + q27::cx(i), y2 = py + q27::cy(i), z2 = pz + q27::cz(i);
+                        if (solid_at(st.rot, x2, y2, z2) || solid_at(st.rot_prev, x2, y2, z2)) continue;
+                        const Mom mo = moments(own(l, st.src, cidx(l, (uint32_t)x2, (uint32_t)y2, (uint32_t)z2)));
+                        const Real r2 = (Real)1 + mo.rho1;
+                        const Real u2[3] = {mo.j[0] / r2, mo.j[1] / r2, mo.j[2] / r2};
+                        Real ps[6];
+                        stress(mo, r2, u2, ps);
+                        for (int c = 0; c < 6; c++) pis[c] += ps[c];
+                        rs += r2;
+                        cnt += 1;
+                    }
+                    const Real rho = cnt > 0 ? rs / cnt : (Real)1;
+                    if (cnt > 0)
+                        for (int c = 0; c < 6; c++) pis[c] /= cnt;
+                    const Real uw[3] = {st.omega[1] * pc[2] - st.omega[2] * pc[1], st.omega[2] * pc[0] - st.omega[0] * pc[2],
+                                        st.omega[0] * pc[1] - st.omega[1] * pc[0]};
+                    put(l, st.src, n, rebuild(rho, uw, pis), st.seed);
+                    for (int c = 0; c < 3; c++) Fv[c] = -rho * uw[c];
+                }
+                l.flags[n] = (k + 1u) << 3;
+            }
+            Real *ft = &rec_ft[(size_t)k * 6];
+            for (int c = 0; c < 3; c++) ft[c] = Fv[c];
+            ft[3] = pc[1] * Fv[2] - pc[2] * Fv[1];
+            ft[4] = pc[2] * Fv[0] - pc[0] * Fv[2];
+            ft[5] = pc[0] * Fv[1] - pc[1] * Fv[0];
+            for (int c = 0; c < 6; c++) w[q27::R_FT + c] = fbits((float)ft[c]);
+        }
+        for (size_t j = 0; j < qscr.size(); j += 3) { qscr[j] = 0x7f7fffffu; qscr[j + 1] = 0; qscr[j + 2] = 0; }
+    }
+
     std::array<double, 6> reduce() const {
         std::array<double, 6> v{};
         for (uint32_t r = 0; r < nrec; r++)
@@ -702,7 +917,11 @@ struct Multi27 {
         base.seed = seed_of(hslot, lsrc, lmw);
         if (sin)
             for (int k = 0; k < 3; k++) base.omega[k] = sizeof(Real) == 8 ? (Real)sin->omega[k] : (Real)(float)sin->omega[k];
+        if (sin)
+            for (int r = 0; r < 3; r++)
+                for (int c = 0; c < 3; c++) { base.rot[3 * r + c] = (float)sin->rot[r][c]; base.rot_prev[3 * r + c] = (float)sin->rot_prev[r][c]; }
         if (l == 0 && !lv[0].faces.empty()) face_bc(lv[0], base);
+        if (moving && l == finest) revoxel(lv[l], base);
         step(l, base);
         lv[l].src = 1u - lsrc;
         lv[l].mslot = lmw;

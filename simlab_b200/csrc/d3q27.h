@@ -53,6 +53,18 @@ struct LevelParams {
     double *recd;               // FP64 engine: 6 doubles (F, T) per record
     uint32_t nrec;
     float4 *dump;
+    // a spinning part on this (finest) level: every swept-box cell is a
+    // record, re-voxelized each finest step from the step's rotation
+    int moving;
+    const uint32_t *occ;        // body-frame occupancy bits
+    float occ_lo[3];
+    float occ_invh;
+    int32_t occ_n[3];
+    const float4 *tris;         // 3 per triangle: v0, e1, e2 (body frame)
+    uint32_t ntri;
+    int32_t box_lo[3];
+    uint32_t box_n[3];
+    uint32_t *qscr;             // 13 positive links x (nearest t, farthest t, hits) per box cell
     Consts27<float> kf;
     Consts27<double> kd;
 };
@@ -65,6 +77,8 @@ struct StepArgs {
     float blend;        // ghost fill: time fraction between mold and mnew
     float omega[3];     // wall angular velocity, rad per finest step
     double omega_d[3];
+    float rot[9];       // body axes in lattice coordinates (row-major, columns = axes)
+    float rot_prev[9];  // the same one finest step earlier
 };
 
 // storage: lbm_storage (0 FP32, 1 FP16, 2 BF16, 3 FP64)
@@ -79,5 +93,7 @@ cudaError_t launch27_mass(int storage, const LevelParams &p, uint32_t src, doubl
 // order: per-block partials, the last block sums them)
 cudaError_t launch27_reduce(const LevelParams &p, int fp64, double *partials, uint32_t *ticket, double *out, cudaStream_t st);
 uint32_t reduce27_blocks(uint32_t nrec);
+// re-voxelize the spinning part's swept box for the rotation in `a` (finest level)
+cudaError_t launch27_revoxel(int storage, const LevelParams &p, const StepArgs &a, cudaStream_t st);
 
 }  // namespace lbm27

@@ -26,6 +26,7 @@
 #include <type_traits>
 
 #include "d3q27.h"
+#include "spin_math.cuh"
 
 namespace lbm27 {
 
@@ -391,6 +392,13 @@ __global__ void __launch_bounds__(BLK, StepOcc<S, WRAP>::value) k27_step(const _
             Tv[1] += xw[2] * flk[0] - xw[0] * flk[2];
             Tv[2] += xw[0] * flk[1] - xw[1] * flk[0];
         }
+        if (p.moving) {
+            // plus what the re-voxelizer booked for this cell this step
+            for (int c = 0; c < 3; c++) {
+                Fv[c] += p.recd ? (R)p.recd[r * 6 + c] : (R)__uint_as_float(p.recs[r * RS + R_FT + c]);
+                Tv[c] += p.recd ? (R)p.recd[r * 6 + 3 + c] : (R)__uint_as_float(p.recs[r * RS + R_FT + 3 + c]);
+            }
+        }
         for (int c = 0; c < 3; c++) {
             p.recs[r * RS + R_FT + c] = __float_as_uint((float)Fv[c]);
             p.recs[r * RS + R_FT + 3 + c] = __float_as_uint((float)Tv[c]);
@@ -679,6 +687,185 @@ __global__ void __launch_bounds__(BLK) k27_mass(const __grid_constant__ LevelPar
     }
 }
 
+// ------------------------------------------------------------ spinning part
+// The D3Q19 re-voxelizer (crates/cfd/src/shader.rs:865-1104) carried to the 27
+// directions of this lattice (the reference spins parts on D3Q19 only): each
+// link is kept once, at the cell it leaves along one of the 13 directions
+// i = 14..26 (the partner -c of each has index 26 - i < 13).  In the pull
+// scheme a just-uncovered cell's refill is written straight into the source
+// set, where its neighbours pull it this step.
+namespace sp27 {
+using namespace lbm::rv;
+__device__ __forceinline__ bool solid(const LevelParams &p, const float *rot, int x, int y, int z) {
+    const V3 pc = {fs((float)x, p.kf.center[0]), fs((float)y, p.kf.center[1]), fs((float)z, p.kf.center[2])};
+    return occ_bit(p.occ, p.occ_lo, p.occ_invh, p.occ_n, to_body(rot, pc));
+}
+__device__ __forceinline__ bool in_box(const LevelParams &p, int lx, int ly, int lz) {
+    return lx >= 0 && ly >= 0 && lz >= 0 && lx < (int)p.box_n[0] && ly < (int)p.box_n[1] && lz < (int)p.box_n[2];
+}
+}  // namespace sp27
+
+__global__ void __launch_bounds__(BLK) k27_tri_scatter(const __grid_constant__ LevelParams p, const StepArgs a) {
+    using namespace lbm::rv;
+    const uint32_t t = blockIdx.x * BLK + threadIdx.x;
+    if (t >= p.ntri) return;
+    const float4 t0 = p.tris[3 * t], t1 = p.tris[3 * t + 1], t2 = p.tris[3 * t + 2];
+    const V3 ctr = {p.kf.center[0], p.kf.center[1], p.kf.center[2]};
+    const V3 va = add(ctr, from_body(a.rot, {t0.x, t0.y, t0.z}));
+    const V3 e1 = from_body(a.rot, {t1.x, t1.y, t1.z});
+    const V3 e2 = from_body(a.rot, {t2.x, t2.y, t2.z});
+    const V3 nrm = cross(e1, e2);
+    const float nl = __fsqrt_rn(dot(nrm, nrm));
+    if (nl < 1e-12f) return;
+    const V3 nn = {__fdiv_rn(nrm.x, nl), __fdiv_rn(nrm.y, nl), __fdiv_rn(nrm.z, nl)};
+    const V3 vb = add(va, e1), vc = add(va, e2);
+    constexpr float REACH = 1.733f;  // the longest link, sqrt(3)
+    const float mn[3] = {fminf(fminf(va.x, vb.x), vc.x), fminf(fminf(va.y, vb.y), vc.y), fminf(fminf(va.z, vb.z), vc.z)};
+    const float mx[3] = {fmaxf(fmaxf(va.x, vb.x), vc.x), fmaxf(fmaxf(va.y, vb.y), vc.y), fmaxf(fmaxf(va.z, vb.z), vc.z)};
+    int lo[3], hi[3];
+    for (int c = 0; c < 3; c++) {
+        lo[c] = max((int)ceilf(fs(mn[c], REACH)), p.box_lo[c]);
+        hi[c] = min((int)floorf(fa(mx[c], REACH)), p.box_lo[c] + (int)p.box_n[c] - 1);
+    }
+    for (int z = lo[2]; z <= hi[2]; z++)
+        for (int y = lo[1]; y <= hi[1]; y++)
+            for (int x = lo[0]; x <= hi[0]; x++) {
+                const V3 pt = {(float)x, (float)y, (float)z};
+                const float d0 = dot(nn, sub(pt, va));
+                if (fabsf(d0) > REACH) continue;
+                const uint32_t k = ((uint32_t)(z - p.box_lo[2]) * p.box_n[1] + (uint32_t)(y - p.box_lo[1])) * p.box_n[0] + (uint32_t)(x - p.box_lo[0]);
+#pragma unroll
+                for (int i = 14; i < 27; i++) {
+                    const V3 cv = {(float)CX(i), (float)CY(i), (float)CZ(i)};
+                    const float d1 = fa(d0, dot(nn, cv));
+                    if (fm(d0, d1) > 0.0f && fabsf(d0) > 1e-6f) continue;
+                    const float tt = ray_tri(pt, cv, va, e1, e2);
+                    if (tt <= 1.0f) {
+                        const uint64_t o = ((uint64_t)k * 13u + (uint32_t)(i - 14)) * 3u;
+                        const uint32_t tb = __float_as_uint(tt > 0.0f ? tt : 0.0f);
+                        atomicMin(p.qscr + o, tb);
+                        atomicMax(p.qscr + o + 1, tb);
+                        atomicAdd(p.qscr + o + 2, 1u);
+                    }
+                }
+            }
+}
+
+__global__ void __launch_bounds__(BLK) k27_qclear(const __grid_constant__ LevelParams p) {
+    const uint64_t k = (uint64_t)blockIdx.x * BLK + threadIdx.x;
+    if (k >= (uint64_t)p.nrec * 13u) return;
+    p.qscr[3 * k] = 0x7f7fffffu;
+    p.qscr[3 * k + 1] = 0u;
+    p.qscr[3 * k + 2] = 0u;
+}
+
+template <class S>
+__global__ void __launch_bounds__(BLK) k27_voxelize(const __grid_constant__ LevelParams p, const StepArgs a) {
+    using namespace lbm::rv;
+    using R = typename Pop<S>::real;
+    const uint32_t k = blockIdx.x * BLK + threadIdx.x;
+    if (k >= p.nrec) return;
+    const int lx = (int)(k % p.box_n[0]), ly = (int)((k / p.box_n[0]) % p.box_n[1]), lz = (int)(k / (p.box_n[0] * p.box_n[1]));
+    const int px = lx + p.box_lo[0], py = ly + p.box_lo[1], pz = lz + p.box_lo[2];
+    const uint32_t n = ((uint32_t)pz * p.NY + (uint32_t)py) * p.NX + (uint32_t)px;
+    const Consts27<R> &kk = K<R>(p);
+    const R pc[3] = {(R)px - kk.center[0], (R)py - kk.center[1], (R)pz - kk.center[2]};
+    const bool solid_now = sp27::solid(p, a.rot, px, py, pz), solid_before = sp27::solid(p, a.rot_prev, px, py, pz);
+    R F[3] = {0, 0, 0};
+    if (solid_now) {
+        p.flags[n] = T_SOLID | ((k + 1u) << 3);
+        p.recs[k * RS + R_MASK] = 0u;
+        if (!solid_before) {
+            // covered this step: the part takes the cell's momentum
+            R f[27];
+            own<S>(p, a.src, n, f);
+            const Mom<R> mo = moments<R>(f);
+            for (int c = 0; c < 3; c++) F[c] = mo.j[c];
+        }
+    } else {
+        float qv[27], qx[27];
+        uint32_t nh[27];
+#pragma unroll
+        for (int i = 0; i < 27; i++) {
+            qv[i] = 9.0f; qx[i] = -1.0f; nh[i] = 0u;
+            if (i == 13) continue;
+            if (i > 13) {
+                const uint64_t o = ((uint64_t)k * 13u + (uint32_t)(i - 14)) * 3u;
+                const uint32_t c = p.qscr[o + 2];
+                if (c) { qv[i] = __uint_as_float(p.qscr[o]); qx[i] = __uint_as_float(p.qscr[o + 1]); nh[i] = c; }
+            } else if (sp27::in_box(p, lx + CX(i), ly + CY(i), lz + CZ(i))) {
+                const uint32_t k2 = ((uint32_t)(lz + CZ(i)) * p.box_n[1] + (uint32_t)(ly + CY(i))) * p.box_n[0] + (uint32_t)(lx + CX(i));
+                const uint64_t o = ((uint64_t)k2 * 13u + (uint32_t)(26 - i - 14)) * 3u;
+                const uint32_t c = p.qscr[o + 2];
+                if (c) { qv[i] = fs(1.0f, __uint_as_float(p.qscr[o + 1])); qx[i] = fs(1.0f, __uint_as_float(p.qscr[o])); nh[i] = c; }
+            }
+        }
+        uint32_t mask = 0;
+#pragma unroll
+        for (int i = 0; i < 27; i++) {
+            if (i == 13) continue;
+            if (sp27::solid(p, a.rot, px + CX(i), py + CY(i), pz + CZ(i))) {
+                if (nh[i] == 0u) qv[i] = 1.0f;
+                mask |= 1u << i;
+            } else if (nh[i] >= 2u && fs(qx[i], qv[i]) > 1e-5f) {
+                mask |= 1u << i;
+            } else {
+                qv[i] = 1.0f;
+            }
+        }
+#pragma unroll
+        for (int w = 0; w < 13; w++) {
+            const int i0 = 2 * w < 13 ? 2 * w : 2 * w + 1, i1 = 2 * w + 1 < 13 ? 2 * w + 1 : 2 * w + 2;  // slots 2w, 2w+1
+            const uint32_t lo = __half_as_ushort(__float2half_rn(fminf(qv[i0], 1.0f)));
+            const uint32_t hi = __half_as_ushort(__float2half_rn(fminf(qv[i1], 1.0f)));
+            p.recs[k * RS + R_Q + w] = lo | (hi << 16);
+        }
+        p.recs[k * RS + R_MASK] = mask;
+        if (solid_before) {
+            // uncovered this step: a post-collision state at the wall velocity
+            // with the density and the mean non-equilibrium stress of the
+            // neighbours that were fluid before and are now, written to the
+            // source set its neighbours pull from; the part gives up its momentum
+            R rs = 0, cnt = 0, pis[6] = {0, 0, 0, 0, 0, 0};
+            for (int i = 0; i < 27; i++) {
+                if (i == 13) continue;
+                const int qx2 = px + CX(i), qy2 = py + CY(i), qz2 = pz + CZ(i);
+                if (sp27::solid(p, a.rot, qx2, qy2, qz2) || sp27::solid(p, a.rot_prev, qx2, qy2, qz2)) continue;
+                R f[27];
+                own<S>(p, a.src, ((uint32_t)qz2 * p.NY + (uint32_t)qy2) * p.NX + (uint32_t)qx2, f);
+                const Mom<R> mo = moments<R>(f);
+                const R r2 = (R)1 + mo.rho1;
+                const R u2[3] = {mo.j[0] / r2, mo.j[1] / r2, mo.j[2] / r2};
+                R ps[6];
+                stress<R>(mo, r2, u2, ps);
+                for (int c = 0; c < 6; c++) pis[c] += ps[c];
+                rs += r2;
+                cnt += (R)1;
+            }
+            const R rho = cnt > (R)0 ? rs / cnt : (R)1;
+            if (cnt > (R)0)
+                for (int c = 0; c < 6; c++) pis[c] /= cnt;
+            R om[3];
+            if (sizeof(R) == 8) { om[0] = (R)a.omega_d[0]; om[1] = (R)a.omega_d[1]; om[2] = (R)a.omega_d[2]; }
+            else { om[0] = (R)a.omega[0]; om[1] = (R)a.omega[1]; om[2] = (R)a.omega[2]; }
+            const R uw[3] = {om[1] * pc[2] - om[2] * pc[1], om[2] * pc[0] - om[0] * pc[2], om[0] * pc[1] - om[1] * pc[0]};
+            R f[27];
+            rebuild<R>(rho, uw, pis, f);
+            Rng rng = cell_rng<S>(n, a.seed_mix);
+            put<S>(p, a.src, n, f, rng);
+            for (int c = 0; c < 3; c++) F[c] = -rho * uw[c];
+        }
+        p.flags[n] = (k + 1u) << 3;
+    }
+    const R T[3] = {pc[1] * F[2] - pc[2] * F[1], pc[2] * F[0] - pc[0] * F[2], pc[0] * F[1] - pc[1] * F[0]};
+    for (int c = 0; c < 3; c++) {
+        p.recs[k * RS + R_FT + c] = __float_as_uint((float)F[c]);
+        p.recs[k * RS + R_FT + 3 + c] = __float_as_uint((float)T[c]);
+    }
+    if (p.recd)
+        for (int c = 0; c < 3; c++) { p.recd[k * 6 + c] = (double)F[c]; p.recd[k * 6 + 3 + c] = (double)T[c]; }
+}
+
 // FP64 sum of the records' force and moment: per-block partials in fixed
 // order, the last block to finish sums the partials (mshader.rs:519-562 does
 // the same sum in f32)
@@ -807,6 +994,19 @@ cudaError_t launch27_mass(int storage, const LevelParams &p, uint32_t src, doubl
 }
 
 uint32_t reduce27_blocks(uint32_t nrec) { return (nrec + RED_BLK - 1) / RED_BLK; }
+
+cudaError_t launch27_revoxel(int storage, const LevelParams &p, const StepArgs &a, cudaStream_t st) {
+    if (!p.moving) return cudaSuccess;
+    if (p.ntri) k27_tri_scatter<<<blocks_for(p.ntri), BLK, 0, st>>>(p, a);
+    cudaError_t e = dispatch(storage, [&](auto *t) {
+        using S = std::remove_pointer_t<decltype(t)>;
+        k27_voxelize<S><<<blocks_for(p.nrec), BLK, 0, st>>>(p, a);
+        return cudaGetLastError();
+    });
+    if (e != cudaSuccess) return e;
+    k27_qclear<<<blocks_for((uint64_t)p.nrec * 13u), BLK, 0, st>>>(p);
+    return cudaGetLastError();
+}
 
 cudaError_t launch27_reduce(const LevelParams &p, int fp64, double *partials, uint32_t *ticket, double *out, cudaStream_t st) {
     if (p.nrec == 0) return cudaMemsetAsync(out, 0, 6 * sizeof(double), st);

@@ -811,7 +811,7 @@ static const uint64_t STATE_MAGIC = 0x4c424d5354415431ull;
 int lbm_state_size(const lbm_lattice *h, uint64_t *bytes) {
     if (!h || !bytes) return LBM_ERR_INVALID;
     *bytes = sizeof(StateHeader) + 19 * h->lp.NP * storage_bytes(h->setup.storage) + (uint64_t)h->nrec * lbm::RS * 4 +
-             (h->lp.recd ? (uint64_t)h->nrec * lbm::RD * 8 : 0);
+             (h->lp.recd ? (uint64_t)h->nrec * lbm::RD * 8 : 0) + (h->lp.moving ? (uint64_t)h->lp.N * 4 : 0);  // a spinning part's flags change
     return LBM_OK;
 }
 
@@ -831,6 +831,8 @@ int lbm_save_state(lbm_lattice *h, void *buf, uint64_t bytes) {
         if (h->nrec) ck(cudaMemcpyAsync(o, h->lp.recs, (size_t)h->nrec * lbm::RS * 4, cudaMemcpyDeviceToHost, h->stream), "state readback");
         o += (size_t)h->nrec * lbm::RS * 4;
         if (h->lp.recd && h->nrec) ck(cudaMemcpyAsync(o, h->lp.recd, (size_t)h->nrec * lbm::RD * 8, cudaMemcpyDeviceToHost, h->stream), "state readback");
+        o += h->lp.recd ? (size_t)h->nrec * lbm::RD * 8 : 0;
+        if (h->lp.moving) ck(cudaMemcpyAsync(o, h->lp.flags, (size_t)h->lp.N * 4, cudaMemcpyDeviceToHost, h->stream), "state readback");
         h->wait();
     });
 }
@@ -852,6 +854,8 @@ int lbm_load_state(lbm_lattice *h, const void *buf, uint64_t bytes) {
         if (h->nrec) ck(cudaMemcpyAsync(h->lp.recs, o, (size_t)h->nrec * lbm::RS * 4, cudaMemcpyHostToDevice, h->stream), "state upload");
         o += (size_t)h->nrec * lbm::RS * 4;
         if (h->lp.recd && h->nrec) ck(cudaMemcpyAsync(h->lp.recd, o, (size_t)h->nrec * lbm::RD * 8, cudaMemcpyHostToDevice, h->stream), "state upload");
+        o += h->lp.recd ? (size_t)h->nrec * lbm::RD * 8 : 0;
+        if (h->lp.moving) ck(cudaMemcpyAsync(h->lp.flags, o, (size_t)h->lp.N * 4, cudaMemcpyHostToDevice, h->stream), "state upload");
         h->wait();
         h->steps_done = hd.steps_done;
         // the blob holds the fused x faces' slots when its step wrote them

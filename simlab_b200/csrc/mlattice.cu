@@ -135,9 +135,17 @@ struct lbm_multi {
         a.src = lsrc;
         a.mw = lmw;
         a.seed_mix = mix(seed_of(hslot, lsrc, lmw));
-        if (l == finest && fine)
+        for (int k = 0; k < 9; k++) a.rot[k] = a.rot_prev[k] = (k % 4 == 0) ? 1.0f : 0.0f;
+        if (l == finest && fine) {
             for (int k = 0; k < 3; k++) { a.omega[k] = (float)fine[fine_i].omega[k]; a.omega_d[k] = fine[fine_i].omega[k]; }
+            for (int r = 0; r < 3; r++)
+                for (int c = 0; c < 3; c++) {
+                    a.rot[3 * r + c] = (float)fine[fine_i].rot[r][c];
+                    a.rot_prev[3 * r + c] = (float)fine[fine_i].rot_prev[r][c];
+                }
+        }
         if (l == 0) ck(lbm27::launch27_face(storage, L.p, a, stream), "face kernel");
+        if (L.p.moving) ck(lbm27::launch27_revoxel(storage, L.p, a, stream), "re-voxelizer");
         ck(lbm27::launch27_step(storage, L.p, a, stream), "step kernel");
         L.src = 1u - lsrc;
         L.mslot = lmw;
@@ -258,7 +266,7 @@ void create_multi(const lbm_multi_setup *setup, const lbm_geometry *geom, const 
         if (p0 != p1) throw MErr(LBM_ERR_INVALID, "periodic faces must come in pairs");
         per0[a] = p0;
     }
-    if (geom && geom->kind != 0 && geom->kind != 1) throw MErr(LBM_ERR_UNSUPPORTED, "only static geometry is supported by this lattice");
+    if (geom && (geom->kind < 0 || geom->kind > 2)) throw MErr(LBM_ERR_INVALID, "unknown geometry kind");
     if (probes && (probes->nvert || probes->nslices))
         throw MErr(LBM_ERR_UNSUPPORTED, "vertex and slice probes are not available on the multi-level lattice");
     if (s.dims0[0] < 3 || s.dims0[1] < 3 || s.dims0[2] < 3) throw MErr(LBM_ERR_INVALID, "grid must be at least 3 cells in every direction");
@@ -293,6 +301,35 @@ void create_multi(const lbm_multi_setup *setup, const lbm_geometry *geom, const 
     }
     const auto fd = dims(finest);
     const uint64_t NF = (uint64_t)fd[0] * fd[1] * fd[2];
+
+    // A spinning part on the finest level (no counterpart: the reference
+    // spins parts on D3Q19 only): every swept-box cell is a record without
+    // links, re-voxelized each finest step.
+    const lbm_geometry *spin = (geom && geom->kind == 2) ? geom : nullptr;
+    std::vector<lbm_wall_cell> boxwalls;
+    lbm_geometry boxgeom{};
+    if (spin) {
+        for (int k = 0; k < 3; k++)
+            if (spin->box_lo[k] < 1 || (int64_t)spin->box_lo[k] + (int64_t)spin->box_n[k] > (int64_t)fd[k] - 1 || spin->box_n[k] == 0)
+                throw MErr(LBM_ERR_INVALID, "the spinning part's swept box leaves the finest level");
+        if (!spin->occ_bits || (spin->ntri && !spin->tris) || !(spin->occ_h > 0.0))
+            throw MErr(LBM_ERR_INVALID, "spinning part without occupancy grid or triangles");
+        const uint64_t nb = (uint64_t)spin->box_n[0] * spin->box_n[1] * spin->box_n[2];
+        if (nb >= 0x1fffffffull || spin->ntri >= 0x7fffffffull) throw MErr(LBM_ERR_INVALID, "swept box too large");
+        boxwalls.resize(nb);
+        uint64_t k = 0;
+        for (uint32_t z = 0; z < spin->box_n[2]; z++)
+            for (uint32_t y = 0; y < spin->box_n[1]; y++)
+                for (uint32_t x = 0; x < spin->box_n[0]; x++, k++) {
+                    boxwalls[k].cell = (uint32_t)((((uint64_t)z + spin->box_lo[2]) * fd[1] + (uint64_t)y + spin->box_lo[1]) * fd[0] + (uint64_t)x + spin->box_lo[0]);
+                    boxwalls[k].mask = 0;
+                    for (int i = 0; i < 27; i++) boxwalls[k].q[i] = 1.0f;
+                }
+        boxgeom.kind = 1;
+        boxgeom.walls = boxwalls.data();
+        boxgeom.nwalls = nb;
+        geom = &boxgeom;
+    }
 
     // records (mlattice.rs:178-192, 345-354): words in the reference layout
     const bool stat = geom && geom->kind == 1;
@@ -444,6 +481,28 @@ void create_multi(const lbm_multi_setup *setup, const lbm_geometry *geom, const 
     h->mass_d = (double *)h->dalloc(16);
     h->bad_d = (unsigned long long *)h->dalloc(16);
     if (s.debug_dump) h->dump = (float4 *)h->dalloc(max_n * sizeof(float4));
+    if (spin) {
+        lbm27::LevelParams &p = h->lv[finest].p;
+        p.moving = 1;
+        const uint64_t nocc = (uint64_t)spin->occ_dims[0] * spin->occ_dims[1] * spin->occ_dims[2];
+        const uint64_t wocc = (nocc + 31) / 32;
+        p.occ = (const uint32_t *)h->dalloc(wocc * 4);
+        ck(cudaMemcpy((void *)p.occ, spin->occ_bits, wocc * 4, cudaMemcpyHostToDevice), "upload occupancy");
+        for (int k = 0; k < 3; k++) {
+            p.occ_lo[k] = (float)spin->occ_lo[k];
+            p.occ_n[k] = (int32_t)spin->occ_dims[k];
+            p.box_lo[k] = spin->box_lo[k];
+            p.box_n[k] = spin->box_n[k];
+        }
+        p.occ_invh = (float)(1.0 / spin->occ_h);
+        p.ntri = (uint32_t)spin->ntri;
+        p.tris = (const float4 *)h->dalloc(std::max<uint64_t>(spin->ntri, 1) * 48);
+        if (spin->ntri) ck(cudaMemcpy((void *)p.tris, spin->tris, spin->ntri * 48, cudaMemcpyHostToDevice), "upload triangles");
+        std::vector<uint32_t> q0((size_t)h->nrec * 39, 0u);
+        for (size_t k = 0; k < q0.size(); k += 3) q0[k] = 0x7f7fffffu;  // nearest hit: FLT_MAX
+        p.qscr = (uint32_t *)h->dalloc(q0.size() * 4);
+        ck(cudaMemcpy(p.qscr, q0.data(), q0.size() * 4, cudaMemcpyHostToDevice), "upload link scratch");
+    }
     for (size_t l = 0; l < nl; l++) {
         lbm27::LevelParams &p = h->lv[l].p;
         p.dump = h->dump;

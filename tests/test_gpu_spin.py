@@ -108,3 +108,14 @@ def test_spinning_part_mass_follows_the_oracle():
     mo = o.macros()
     assert bad == 0
     assert abs(m1 / np.nansum(mo[:, 0]) - 1.0) < 1e-9
+
+
+def test_spinning_checkpoint_round_trip_is_exact():
+    st, geo = spin_case(Storage.FP16)
+    g = Lattice(st, geo)
+    g.run(spin_steps(13, 0.02))
+    blob = g.save_state()
+    a = g.run(spin_steps(21, 0.02, a0=13 * 0.02))
+    g.load_state(blob)
+    b = g.run(spin_steps(21, 0.02, a0=13 * 0.02))
+    assert np.array_equal(a, b)
