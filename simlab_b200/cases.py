@@ -13,6 +13,11 @@ smoke check and the bench.
   open outlet and sides; tunnel.rs:764-771) with sponges 16/32/16 cells,
   sponge tau 1.0 and absorbing strength 0.1 (tunnel.rs:206-234, 1006-1007).
   `scale=2` gives the 1024x512x512 arm.
+* `prop_refined`: D3Q27 cumulant on three nested levels (coarse 256x128x128,
+  each finer box 0.63 of its parent per axis, about a quarter of its volume)
+  with a 2-blade rotor of radius 60 finest cells spinning on the finest level
+  (chord 0.15R -> 0.08R, twist 25 -> 8 degrees, 5 % elliptic section), tip
+  speed 0.08, axial inflow 0.02, spin-up over half a revolution.
 * `gray_design`: the gray-level adjoint case, 192x96x96 D3Q19 BGK with a
   64x48x48 design box of smoothed random solid fraction, drag averaged over
   steps 500-1000, a checkpoint every 50 steps.
@@ -115,3 +120,69 @@ def gray_design(storage=Storage.FP32, dims=(192, 96, 96), box_lo=(48, 24, 24), b
     st = GraySetup(dims=list(dims), box_lo=list(box_lo), box_n=list(box_n), nu=nu, u_in=[u, 0.0, 0.0], alpha=1.0, center=center, storage=storage)
     spec = AdjointSpec(steps=1000, t0=500, t1=1000, checkpoint_every=50, objective=0, dir=[1.0, 0.0, 0.0], recompute=True)
     return st, g, spec
+
+
+# ------------------------------------------------------------------ refined rotor case
+def rotation(axis, theta):
+    """Rotation by theta about a unit axis (Rodrigues)."""
+    a = np.asarray(axis, dtype=np.float64)
+    a = a / np.linalg.norm(a)
+    K = np.array([[0, -a[2], a[1]], [a[2], 0, -a[0]], [-a[1], a[0], 0]])
+    return np.eye(3) + np.sin(theta) * K + (1 - np.cos(theta)) * (K @ K)
+
+
+# body frame -> lattice: the rotor's spin axis (body z) along the tunnel flow (lattice x)
+BODY_TO_LATTICE = np.array([[0.0, 0.0, 1.0], [1.0, 0.0, 0.0], [0.0, 1.0, 0.0]])
+
+
+def spin_schedule(n, omega, ramp_steps, axis=(1.0, 0.0, 0.0), body=BODY_TO_LATTICE, start=0):
+    """StepIn records of a part spinning about the lattice `axis` at `omega`
+    rad per finest step, spun up with the smoothstep of tunnel.rs:1085-1098
+    over `ramp_steps`: rot is the body->lattice rotation after each step,
+    rot_prev the one before, omega the step's angular velocity."""
+    from .lbm import steps_array
+
+    a = steps_array(n)
+    ax = np.asarray(axis, dtype=np.float64)
+    theta = 0.0
+    prev = body.copy()
+    for s in range(start + n):
+        x = (s + 0.5) / ramp_steps if s < ramp_steps else 1.0
+        f = x * x * (3.0 - 2.0 * x) if s < ramp_steps else 1.0
+        theta += f * omega
+        rot = rotation(ax, theta) @ body
+        if s >= start:
+            k = s - start
+            a[k]["rot"] = rot
+            a[k]["rot_prev"] = prev
+            a[k]["omega"] = ax * (f * omega)
+        prev = rot
+    return a
+
+
+def prop_refined(storage=Storage.FP32, radius=60.0, tip_speed=0.08, u=0.02, nu_finest=4e-5, dims0=(256, 128, 128), sponge=True):
+    """The refined rotor case: returns (MultiSetup, SpinGeometry, omega).
+    The rotor sits at the centre of the finest level (plus sub-cell offsets
+    so no symmetry plane falls on a lattice plane), its axis along the flow."""
+    from .lbm import SpinGeometry, voxelize_spin
+    from .mlattice import LevelBox, MultiSetup
+    from .shapes import propeller
+
+    F = FaceBc
+    nl = 3
+    s = MultiSetup(dims0=list(dims0), faces=[F.VELOCITY] + [F.OPEN] * 5, nu0=nu_finest / 2 ** (nl - 1), u_inf=[u, 0.0, 0.0],
+                   u_init=[u, 0.0, 0.0], sponge=[0, 16, 8, 8, 8, 8] if sponge else [0] * 6, sponge_tau=1.0, sponge_sigma=0.1 if sponge else 0.0,
+                   total_pressure_inlet=True, storage=storage, debug_dump=False)
+    for l in range(1, nl):
+        d = s.dims(l - 1)
+        n = [int(d[k] * 0.63) for k in range(3)]
+        s.boxes.append(LevelBox(lo=[(d[k] - n[k]) // 2 for k in range(3)], n=n))
+    fd = s.dims(nl - 1)
+    c = [0.5 * (fd[0] - 1) + 0.31, 0.5 * (fd[1] - 1) + 0.23, 0.5 * (fd[2] - 1) + 0.17]
+    s.center = c
+    v, t = propeller(radius=radius)
+    sv = voxelize_spin(v, t, [0.0, 0.0, 1.0], 0.125)
+    r = int(np.ceil(sv.radius)) + 3
+    ax_lo, ax_hi = int(np.floor(c[0] + sv.axial[0])) - 3, int(np.ceil(c[0] + sv.axial[1])) + 3
+    geo = SpinGeometry(vox=sv, box_lo=[ax_lo, int(c[1]) - r, int(c[2]) - r], box_n=[ax_hi - ax_lo + 1, 2 * r + 2, 2 * r + 2])
+    return s, geo, tip_speed / radius

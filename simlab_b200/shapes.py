@@ -3,7 +3,9 @@
 `cuboid` and `sphere` follow crates/cfd/src/shapes.rs:8-21 and 47-99 (axis-
 aligned box with outward triangles; geodesic sphere from a subdivided
 icosahedron).  `arm` builds the quadcopter-arm stand-in of the 512x256x256
-LES case: a box beam with a cylinder at one end.
+LES case: a box beam with a cylinder at one end.  `propeller` builds the
+parametric rotor of the refined D3Q27 case (linear chord and twist, elliptic
+section, cylindrical hub).
 """
 from __future__ import annotations
 
@@ -105,3 +107,56 @@ def arm(center=(128.0, 128.0, 128.0), length=200.0, width=12.0, thick=8.0, cyl_r
     box = cuboid([cx - W / 2 + 0.013, cy - L / 2 + 0.017, cz - T / 2 + 0.011], [cx + W / 2 + 0.013, cy + L / 2 + 0.017, cz + T / 2 + 0.011])
     cyl = cylinder([cx + 0.013, cy + L / 2 + 0.017, cz + 0.011], cyl_r * scale, cyl_h * scale, axis=2)
     return merge(box, cyl)
+
+
+def blade(radius=60.0, r_root=7.0, chord_root=0.15, chord_tip=0.08, twist_root=25.0, twist_tip=8.0, thick=0.05, nr=48, ns=32):
+    """One blade along +x in body coordinates (spin axis z): stations from
+    r_root to `radius`, chord falling linearly from chord_root * radius to
+    chord_tip * radius, twist (the section's angle to the rotation plane) from
+    twist_root to twist_tip degrees, an elliptic section of thickness
+    `thick` x chord centred on the mid-chord line; outward-facing, capped
+    at both ends.  The blade moves toward +y when the part spins about +z."""
+    verts, tris = [], []
+    for k in range(nr + 1):
+        r = r_root + (radius - r_root) * k / nr
+        f = (r - r_root) / (radius - r_root)
+        c = (chord_root + (chord_tip - chord_root) * f) * radius
+        th = math.radians(twist_root + (twist_tip - twist_root) * f)
+        for j in range(ns):
+            ph = 2.0 * math.pi * j / ns
+            s = 0.5 * c * math.cos(ph)  # chordwise, leading edge at +s
+            t = 0.5 * thick * c * math.sin(ph)
+            # chord along (0, cos th, -sin th), thickness normal (0, sin th, cos th)
+            verts.append([r, s * math.cos(th) + t * math.sin(th), -s * math.sin(th) + t * math.cos(th)])
+    for k in range(nr):
+        for j in range(ns):
+            j1 = (j + 1) % ns
+            a, b = k * ns + j, k * ns + j1
+            c_, d = (k + 1) * ns + j, (k + 1) * ns + j1
+            tris += [[a, b, d], [a, d, c_]]
+    c0 = len(verts)
+    verts.append([r_root, 0.0, 0.0])
+    c1 = len(verts)
+    verts.append([radius, 0.0, 0.0])
+    for j in range(ns):
+        j1 = (j + 1) % ns
+        tris.append([c0, j1, j])
+        tris.append([c1, nr * ns + j, nr * ns + j1])
+    return np.array(verts, dtype=np.float64), np.array(tris, dtype=np.uint32)
+
+
+def propeller(radius=60.0, blades=2, hub_radius=None, hub_height=None, **kw):
+    """A rotor in body coordinates (origin at the centre, spin axis z):
+    `blades` copies of `blade` spaced evenly about z and a cylindrical hub.
+    Defaults: hub radius 0.12 R and height 0.15 R."""
+    hr = 0.12 * radius if hub_radius is None else hub_radius
+    hh = 0.15 * radius if hub_height is None else hub_height
+    bv, bt = blade(radius=radius, r_root=0.8 * hr, **kw)
+    parts = [cylinder([0.0, 0.0, 0.0], hr, hh, axis=2, n=48)]
+    for b in range(blades):
+        a = 2.0 * math.pi * b / blades
+        c, s = math.cos(a), math.sin(a)
+        v = bv.copy()
+        v[:, 0], v[:, 1] = c * bv[:, 0] - s * bv[:, 1], s * bv[:, 0] + c * bv[:, 1]
+        parts.append((v, bt))
+    return merge(*parts)

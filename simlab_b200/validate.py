@@ -8,6 +8,12 @@ storages, so its relative error is that of the mean F_x).
 
     python -m simlab_b200.validate arm [steps] [storages...]
     python -m simlab_b200.validate sphere [steps]
+    python -m simlab_b200.validate prop [revolutions] [storages...]
+
+The rotor case (simlab_b200.cases.prop_refined: three D3Q27 levels, a 2-blade
+rotor spinning on the finest) reports thrust (force along the spin axis) and
+torque (moment about it), averaged over the last revolution, per storage,
+beside the device time.
 
 Prints one JSON line.
 """
@@ -59,8 +65,46 @@ def compare(name: str, make, steps: int, storages):
     return res
 
 
+def run_prop(storage, revs: float, chunk: int = 4096):
+    import math
+
+    from .cases import prop_refined, spin_schedule
+    from .mlattice import MultiLattice
+
+    s, geo, om = prop_refined(storage)
+    lat = MultiLattice(s, geo)
+    ss = lat.sub_steps()
+    per_rev = 2.0 * math.pi / om
+    n = int(round(revs * per_rev / ss)) * ss
+    ramp = int(round(0.5 * per_rev))
+    sched = spin_schedule(n, om, ramp)
+    out = []
+    t0 = time.perf_counter()
+    for k in range(0, n, chunk):
+        out.append(lat.run(sched[k:k + chunk]))
+    dt = time.perf_counter() - t0
+    f = np.concatenate(out)
+    last = f[-int(round(per_rev / ss)) * ss:]
+    cells = lat.level_cells()
+    mlups = sum(c * 2 ** l for l, c in enumerate(cells)) / 2 ** (len(cells) - 1) * n / dt / 1e6
+    lat.close()
+    return {"thrust": float(last[:, 0].mean()), "torque": float(last[:, 3].mean()), "steps": n, "seconds": round(dt, 2), "mlups_wall": round(mlups, 1),
+            "finite": bool(np.all(np.isfinite(f)))}
+
+
 def main() -> None:
     which = sys.argv[1] if len(sys.argv) > 1 else "arm"
+    if which == "prop":
+        revs = float(sys.argv[2]) if len(sys.argv) > 2 else 10.0
+        names = sys.argv[3:] or ["fp32", "fp16"]
+        res = {"case": "prop", "revolutions": revs}
+        for nm in names:
+            res[nm] = run_prop(Storage[nm.upper()], revs)
+        if "fp32" in res and "fp16" in res:
+            res["fp16_thrust_rel_err"] = abs(res["fp16"]["thrust"] / res["fp32"]["thrust"] - 1.0)
+            res["fp16_torque_rel_err"] = abs(res["fp16"]["torque"] / res["fp32"]["torque"] - 1.0)
+        print(json.dumps(res))
+        return
     steps = int(sys.argv[2]) if len(sys.argv) > 2 else (20000 if which == "arm" else 2000)
     names = sys.argv[3:] or ["fp32", "fp16", "bf16"]
     storages = [Storage[n.upper()] for n in names]
