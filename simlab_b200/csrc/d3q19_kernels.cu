@@ -27,6 +27,15 @@
 
 namespace lbm {
 
+// compile-time loop: fn(std::integral_constant<int, I>) for I in [A, B)
+template <int A, int B, class Fn>
+__device__ __forceinline__ void constexpr_for(Fn &&fn) {
+    if constexpr (A < B) {
+        fn(std::integral_constant<int, A>{});
+        constexpr_for<A + 1, B>(fn);
+    }
+}
+
 // ---------------------------------------------------------------- collision
 // Everything of shader.rs:815-847 after the wall links: moments, Smagorinsky
 // tau from |Pi_neq| (825-828), wall model, sponge (832-833), regularized or
@@ -384,11 +393,31 @@ __global__ void __launch_bounds__(BLOCK) k_faces(const __grid_constant__ LatPara
 // (one arrival per compute thread) replace block barriers, so compute warps
 // move on to the next tile while the producer writes the last one back.
 constexpr int CWARPS = 7, CTHREADS = CWARPS * 32;
-template <class S> struct Tile { static constexpr uint32_t cells = sizeof(S) == 2 ? 2 * CTHREADS : CTHREADS; };
+// Tile size (cells per compute thread) and buffers per block.  Measured on
+// the B200 with the 512x256x256 arm case: larger tiles amortise the per-tile
+// handshakes (barrier waits, proxy fences, the producer's bookkeeping); two
+// buffers of 896 (2-byte) or 448 (4-byte) cells leave room for two blocks per
+// SM and still hide each tile's load behind the previous tile's collisions.
+#ifndef LBM_TILE_2B
+#define LBM_TILE_2B 4  // cells per compute thread and tile for 2-byte storage
+#endif
+#ifndef LBM_NBUF_2B
+#define LBM_NBUF_2B 2  // tile buffers per block for 2-byte storage
+#endif
+#ifndef LBM_TILE_4B
+#define LBM_TILE_4B 2  // the same for 4-byte storage
+#endif
+#ifndef LBM_NBUF_4B
+#define LBM_NBUF_4B 2
+#endif
+template <class S> struct Tile {
+    static constexpr uint32_t cells = sizeof(S) == 2 ? LBM_TILE_2B * CTHREADS : (sizeof(S) == 4 ? LBM_TILE_4B * CTHREADS : CTHREADS);
+};
 template <class S> constexpr uint32_t slot_bytes() { return Tile<S>::cells * (uint32_t)sizeof(S) + 16; }
 template <class S> constexpr uint32_t buf_bytes() { return 19 * slot_bytes<S>() + Tile<S>::cells * 4; }
-constexpr int NBUF = 3;  // tile buffers per block: loads run up to two tiles ahead
-template <class S> constexpr uint32_t tma_smem() { return NBUF * buf_bytes<S>() + 128; }  // + alignment slack
+// tile buffers per block: loads run up to NBUF - 1 tiles ahead
+template <class S> struct Nbuf { static constexpr int value = sizeof(S) == 2 ? LBM_NBUF_2B : (sizeof(S) == 4 ? LBM_NBUF_4B : 3); };
+template <class S> constexpr uint32_t tma_smem() { return Nbuf<S>::value * buf_bytes<S>() + 128; }  // + alignment slack
 
 // element offset of plane j's first tile cell in its shared-memory slot
 template <class S, int P>
@@ -571,6 +600,7 @@ __device__ __forceinline__ void zwrap_cell(const LatParams &p, const StepParams 
 template <class S, int P, int COLL, int FEAT>
 __global__ void __launch_bounds__(BLOCK, sizeof(S) == 8 ? 2 : 3) k_bulk_tma(const __grid_constant__ LatParams p, const __grid_constant__ StepParams s) {
     using R = typename Pop<S>::real;
+    constexpr int NBUF = Nbuf<S>::value;
     constexpr uint32_t T = Tile<S>::cells, SLOT = slot_bytes<S>(), BUF = buf_bytes<S>();
     constexpr int64_t E16 = 16 / sizeof(S);
     extern __shared__ __align__(128) uint8_t sm_raw[];
@@ -693,15 +723,16 @@ __global__ void __launch_bounds__(BLOCK, sizeof(S) == 8 ? 2 : 3) k_bulk_tma(cons
             Rng rng{sr_hash_mix(n, s.seed_mix)};
             S out[19];
             if constexpr (SC != 1) {
-                // stochastic rounding noise per value, then one packed
-                // round-toward-zero conversion per pair of outputs
-#pragma unroll
-                for (int i = 0; i < 18; i += 2) {
-                    const uint32_t h2 = cvt_rz_f16x2(sr_noise13(f[i + 1], rng), sr_noise13(f[i], rng));
+                // stochastic rounding noise per value (independent per value),
+                // then one packed round-toward-zero conversion per pair
+                const Weyl wn{rng.s};
+                constexpr_for<0, 9>([&](auto kk) {
+                    constexpr int i = 2 * decltype(kk)::value;
+                    const uint32_t h2 = cvt_rz_f16x2(noise13<i + 1>(f[i + 1], wn), noise13<i>(f[i], wn));
                     out[i] = __ushort_as_half((unsigned short)(h2 & 0xffffu));
                     out[i + 1] = __ushort_as_half((unsigned short)(h2 >> 16));
-                }
-                out[18] = __float2half_rz(sr_noise13(f[18], rng));
+                });
+                out[18] = __float2half_rz(noise13<18>(f[18], wn));
             } else {
 #pragma unroll
                 for (int i = 0; i < 19; i++) out[i] = Pop<S>::enc(f[i], rng);

@@ -453,7 +453,7 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     h->pop_bytes = (19 * NP + guard) * sb;
     p.pop = h->dalloc(h->pop_bytes);
     p.NP = NP;
-    const uint64_t NFL = (N + 1023) / 1024 * 1024 + 1024;  // flags padded past the last tile
+    const uint64_t NFL = (N + 2047) / 2048 * 2048 + 2048;  // flags padded past the last tile (tiles up to 2048 cells)
     p.flags = (uint32_t *)h->dalloc(NFL * 4);
     p.err = (uint32_t *)h->dalloc(16);
     p.recs = (uint32_t *)h->dalloc(nrec * lbm::RS * 4);

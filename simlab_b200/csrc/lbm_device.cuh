@@ -172,6 +172,18 @@ struct Rng {
     }
 };
 
+// Independent noise for the values of one cell: the cell's hash r offset by
+// a multiple of the golden-ratio constant per value.  Each value's noise is
+// uniform on its own; unlike the generator sequence the values carry no
+// dependency chain, so a cell's roundings issue in parallel.
+struct Weyl {
+    uint32_t r;
+    template <int I>
+    __device__ __forceinline__ uint32_t bits13() const { return (r + (uint32_t)I * 0x9E3779B9u) >> 19; }
+};
+template <int I>
+__device__ __forceinline__ float noise13(float v, const Weyl &w) { return __uint_as_float(__float_as_uint(v) + w.bits13<I>()); }
+
 // FP16 stores (f - w) * 32768; 13 random bits below binary16's 10-bit
 // mantissa, then round toward zero (which also saturates at the largest
 // finite half instead of overflowing).
