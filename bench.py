@@ -331,6 +331,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and D3Q27 measurements (launch-list captures)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     ws, rank, local = dist_init()
@@ -405,7 +406,7 @@ def main():
         "gpu_launches": 3 * args.steps,
         "kernel_share": {k: round(v / max(kt["faces_ms"] + kt["walls_ms"] + kt["bulk_ms"], 1e-12), 4) for k, v in kt.items() if k != "steps"},
     }
-    if ws == 1:
+    if ws == 1 and not args.no_extras:
         line["adjoint"] = adjoint_ratio()
         line["d3q27_three_levels_mlups"] = d3q27_levels()
     if rank == 0 and ws == 1 and not args.no_cpu:
