@@ -8,7 +8,7 @@ storages, so its relative error is that of the mean F_x).
 
     python -m simlab_b200.validate arm [steps] [storages...]
     python -m simlab_b200.validate sphere [steps]
-    python -m simlab_b200.validate prop [revolutions] [storages...]
+    python -m simlab_b200.validate prop [revolutions] [storages...] [nu=<finest-level viscosity>]
 
 The rotor case (simlab_b200.cases.prop_refined: three D3Q27 levels, a 2-blade
 rotor spinning on the finest) reports thrust (force along the spin axis) and
@@ -65,13 +65,13 @@ def compare(name: str, make, steps: int, storages):
     return res
 
 
-def run_prop(storage, revs: float, chunk: int = 4096):
+def run_prop(storage, revs: float, chunk: int = 4096, nu_finest: float = 4e-5):
     import math
 
     from .cases import prop_refined, spin_schedule
     from .mlattice import MultiLattice
 
-    s, geo, om = prop_refined(storage)
+    s, geo, om = prop_refined(storage, nu_finest=nu_finest)
     lat = MultiLattice(s, geo)
     ss = lat.sub_steps()
     per_rev = 2.0 * math.pi / om
@@ -96,10 +96,16 @@ def main() -> None:
     which = sys.argv[1] if len(sys.argv) > 1 else "arm"
     if which == "prop":
         revs = float(sys.argv[2]) if len(sys.argv) > 2 else 10.0
-        names = sys.argv[3:] or ["fp32", "fp16"]
-        res = {"case": "prop", "revolutions": revs}
+        rest = sys.argv[3:]
+        nu = 4e-5
+        for a in list(rest):
+            if a.startswith("nu="):
+                nu = float(a[3:])
+                rest.remove(a)
+        names = rest or ["fp32", "fp16"]
+        res = {"case": "prop", "revolutions": revs, "nu_finest": nu}
         for nm in names:
-            res[nm] = run_prop(Storage[nm.upper()], revs)
+            res[nm] = run_prop(Storage[nm.upper()], revs, nu_finest=nu)
         if "fp32" in res and "fp16" in res:
             res["fp16_thrust_rel_err"] = abs(res["fp16"]["thrust"] / res["fp32"]["thrust"] - 1.0)
             res["fp16_torque_rel_err"] = abs(res["fp16"]["torque"] / res["fp32"]["torque"] - 1.0)
