@@ -722,17 +722,20 @@ __global__ void __launch_bounds__(BLOCK, sizeof(S) == 8 ? 2 : 3) k_bulk_tma(cons
             relax<R, COLL, SC, FEAT>(p, k, f, x, y, z, false, 0, 0, 0, 0, 0, om0, rho, ux, uy, uz);
             Rng rng{sr_hash_mix(n, s.seed_mix)};
             S out[19];
-            if constexpr (SC != 1) {
-                // stochastic rounding noise per value (independent per value),
-                // then one packed round-toward-zero conversion per pair
-                const Weyl wn{rng.s};
-                constexpr_for<0, 9>([&](auto kk) {
-                    constexpr int i = 2 * decltype(kk)::value;
-                    const uint32_t h2 = cvt_rz_f16x2(noise13<i + 1>(f[i + 1], wn), noise13<i>(f[i], wn));
-                    out[i] = __ushort_as_half((unsigned short)(h2 & 0xffffu));
-                    out[i + 1] = __ushort_as_half((unsigned short)(h2 >> 16));
+            if constexpr (sizeof(S) == 2) {
+                // two values per stochastically rounding conversion, their
+                // random bits from one product of the cell's hash per pair
+                const uint32_t h = rng.s;
+                constexpr_for<0, 10>([&](auto kk) {
+                    constexpr int K = decltype(kk)::value, i = 2 * K;
+                    if constexpr (i + 1 < 19) {
+                        const uint32_t h2 = Pop<S>::rs2(f[i + 1], f[i], pair_bits<K>(h));
+                        out[i] = Pop<S>::bits(h2 & 0xffffu);
+                        out[i + 1] = Pop<S>::bits(h2 >> 16);
+                    } else {
+                        out[i] = Pop<S>::bits(Pop<S>::rs2(f[i], 0.0f, pair_bits<K>(h)) >> 16);
+                    }
                 });
-                out[18] = __float2half_rz(noise13<18>(f[18], wn));
             } else {
 #pragma unroll
                 for (int i = 0; i < 19; i++) out[i] = Pop<S>::enc(f[i], rng);

@@ -202,7 +202,7 @@ __device__ __forceinline__ Rng cell_rng(uint32_t n, uint32_t seed_mix) {
 // Storage in raw units: FP16 keeps (f - w) * 32768, the others f - w.  The
 // step works on raw loads (no per-population rescale), scales the moments
 // once, and folds the scale back into the last multiply of each output.
-// Stochastic rounding takes two noise fields from each generator step.
+// Stochastic rounding converts two values per generator step.
 template <class S> struct Raw;
 template <> struct Raw<float> {
     static constexpr float SC = 1.0f;
@@ -219,27 +219,26 @@ template <> struct Raw<double> {
 template <> struct Raw<__half> {
     static constexpr float SC = 32768.0f;
     static __device__ __forceinline__ float ld(const __half *p) { return __half2float(*p); }
-    // 13 random bits below binary16's mantissa, then round toward zero
+    // one stochastically rounding conversion per pair
     static __device__ __forceinline__ void st2(__half *a, float va, __half *b, float vb, Rng &r) {
-        const uint32_t x = r.next();
-        *a = __float2half_rz(__uint_as_float(__float_as_uint(va) + (x >> 19)));
-        *b = __float2half_rz(__uint_as_float(__float_as_uint(vb) + ((x >> 6) & 0x1fffu)));
+        const uint32_t h2 = lbm::cvt_rs_f16x2(va, vb, r.next2());
+        *a = __ushort_as_half((unsigned short)(h2 >> 16));
+        *b = __ushort_as_half((unsigned short)(h2 & 0xffffu));
     }
     static __device__ __forceinline__ void st1(__half *a, float va, Rng &r) {
-        *a = __float2half_rz(__uint_as_float(__float_as_uint(va) + (r.next() >> 19)));
+        *a = __ushort_as_half((unsigned short)(lbm::cvt_rs_f16x2(va, 0.0f, r.next()) >> 16));
     }
 };
 template <> struct Raw<__nv_bfloat16> {
     static constexpr float SC = 1.0f;
     static __device__ __forceinline__ float ld(const __nv_bfloat16 *p) { return __bfloat162float(*p); }
-    // 16 random bits below bfloat16's mantissa, then truncate
     static __device__ __forceinline__ void st2(__nv_bfloat16 *a, float va, __nv_bfloat16 *b, float vb, Rng &r) {
-        const uint32_t x = r.next();
-        *a = __ushort_as_bfloat16((unsigned short)((__float_as_uint(va) + (x >> 16)) >> 16));
-        *b = __ushort_as_bfloat16((unsigned short)((__float_as_uint(vb) + (x & 0xffffu)) >> 16));
+        const uint32_t h2 = lbm::cvt_rs_bf16x2(va, vb, r.next2());
+        *a = __ushort_as_bfloat16((unsigned short)(h2 >> 16));
+        *b = __ushort_as_bfloat16((unsigned short)(h2 & 0xffffu));
     }
     static __device__ __forceinline__ void st1(__nv_bfloat16 *a, float va, Rng &r) {
-        *a = __ushort_as_bfloat16((unsigned short)((__float_as_uint(va) + (r.next() >> 16)) >> 16));
+        *a = __ushort_as_bfloat16((unsigned short)(lbm::cvt_rs_bf16x2(va, 0.0f, r.next()) >> 16));
     }
 };
 
