@@ -223,6 +223,14 @@ int lbm_get_kernel_times(lbm_lattice *h, lbm_kernel_times *out);
 /* Host-side limit on device waits, seconds (default 600). */
 int lbm_set_timeout(lbm_lattice *h, double seconds);
 
+/* Self-test of the step kernel's bounded waits (no reference counterpart):
+ * one device thread waits on a bulk-copy barrier phase that nothing completes,
+ * with the kernels' own wait routine and a limit of limit_ns (0 < limit_ns <=
+ * 10 s).  *gave_up = 1 when the wait ended at its limit, as the step kernel's
+ * waits end with LBM_ERR_TIMEOUT instead of hanging; *waited_us = the time it
+ * waited.  No fault and no hang: the device stays usable. */
+int lbm_selftest_copy_wait(uint64_t limit_ns, uint32_t *gave_up, uint64_t *waited_us);
+
 /* Lattice::macros (lattice.rs:818-835): (rho, ux, uy, uz) of every cell,
  * NaN for solid and face cells; needs debug_dump.  out: 4 * cells floats. */
 int lbm_macros(lbm_lattice *h, float *out);

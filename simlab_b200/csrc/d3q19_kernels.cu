@@ -387,36 +387,59 @@ __global__ void __launch_bounds__(BLOCK) k_faces(const __grid_constant__ LatPara
 // flight while the current one is collided).  Every mbarrier wait is
 // bounded; on expiry the block records ERR_COPY_WAIT, drains its copies
 // (bounded) and stops.
-// Warp-specialized: warps 0..6 collide (224 threads), warp 7 is the
-// producer that issues the bulk loads and stores.  Per buffer a "full"
+// Warp-specialized: the first Tma<S>::cwarps warps collide, the last warp is
+// the producer that issues the bulk loads and stores.  Per buffer a "full"
 // mbarrier (producer arrival + transaction bytes) and an "empty" mbarrier
 // (one arrival per compute thread) replace block barriers, so compute warps
 // move on to the next tile while the producer writes the last one back.
-constexpr int CWARPS = 7, CTHREADS = CWARPS * 32;
-// Tile size (cells per compute thread) and buffers per block.  Measured on
-// the B200 with the 512x256x256 arm case: larger tiles amortise the per-tile
-// handshakes (barrier waits, proxy fences, the producer's bookkeeping); two
-// buffers of 896 (2-byte) or 448 (4-byte) cells leave room for two blocks per
-// SM and still hide each tile's load behind the previous tile's collisions.
+// Block shape per storage: compute warps, cells per compute thread and tile,
+// tile buffers, and the blocks per SM the register budget aims at.  Measured
+// on the B200 with the 512x256x256 arm case (MLUPS FP16 / FP32): three blocks
+// of 7 compute warps with 896- / 448-cell tiles 54.9 / 35.3 k; two blocks of
+// 10 warps, 1280 / 640 cells 52.3 / 35.5 k; one block of 20 warps with three
+// buffers of 1280 / 640 cells 46.3 / 34.6 k; one block of 20 warps with two
+// buffers of 2560 / 1280 cells 55.7 / 38.1 k.  The copy engine takes a few
+// hundred cycles per bulk copy (one per plane and tile, each way), so the
+// fewer and larger the copies per SM, the sooner a buffer turns around.
+#ifndef LBM_CWARPS_2B
+#define LBM_CWARPS_2B 20  // compute warps per block for 2-byte storage
+#endif
 #ifndef LBM_TILE_2B
 #define LBM_TILE_2B 4  // cells per compute thread and tile for 2-byte storage
 #endif
 #ifndef LBM_NBUF_2B
 #define LBM_NBUF_2B 2  // tile buffers per block for 2-byte storage
 #endif
+#ifndef LBM_BLOCKS_2B
+#define LBM_BLOCKS_2B 1  // blocks per SM for 2-byte storage
+#endif
+#ifndef LBM_CWARPS_4B
+#define LBM_CWARPS_4B 20  // the same for 4-byte storage
+#endif
 #ifndef LBM_TILE_4B
-#define LBM_TILE_4B 2  // the same for 4-byte storage
+#define LBM_TILE_4B 2
 #endif
 #ifndef LBM_NBUF_4B
 #define LBM_NBUF_4B 2
 #endif
+#ifndef LBM_BLOCKS_4B
+#define LBM_BLOCKS_4B 1
+#endif
+template <class S> struct Tma {
+    static constexpr int cwarps = sizeof(S) == 2 ? LBM_CWARPS_2B : (sizeof(S) == 4 ? LBM_CWARPS_4B : 7);
+    static constexpr int cthreads = cwarps * 32, threads = cthreads + 32;  // + the producer warp
+    static constexpr uint32_t cells = (uint32_t)(sizeof(S) == 2 ? LBM_TILE_2B : (sizeof(S) == 4 ? LBM_TILE_4B : 1)) * cthreads;
+    static constexpr int nbuf = sizeof(S) == 2 ? LBM_NBUF_2B : (sizeof(S) == 4 ? LBM_NBUF_4B : 3);
+    static constexpr int min_blocks = sizeof(S) == 2 ? LBM_BLOCKS_2B : (sizeof(S) == 4 ? LBM_BLOCKS_4B : 2);
+};
 template <class S> struct Tile {
-    static constexpr uint32_t cells = sizeof(S) == 2 ? LBM_TILE_2B * CTHREADS : (sizeof(S) == 4 ? LBM_TILE_4B * CTHREADS : CTHREADS);
+    static constexpr uint32_t cells = Tma<S>::cells;
+    static_assert(cells <= TILE_MAX, "the allocations' guards cover tiles up to TILE_MAX cells");
 };
 template <class S> constexpr uint32_t slot_bytes() { return Tile<S>::cells * (uint32_t)sizeof(S) + 16; }
 template <class S> constexpr uint32_t buf_bytes() { return 19 * slot_bytes<S>() + Tile<S>::cells * 4; }
 // tile buffers per block: loads run up to NBUF - 1 tiles ahead
-template <class S> struct Nbuf { static constexpr int value = sizeof(S) == 2 ? LBM_NBUF_2B : (sizeof(S) == 4 ? LBM_NBUF_4B : 3); };
+template <class S> struct Nbuf { static constexpr int value = Tma<S>::nbuf; };
 template <class S> constexpr uint32_t tma_smem() { return Nbuf<S>::value * buf_bytes<S>() + 128; }  // + alignment slack
 
 // element offset of plane j's first tile cell in its shared-memory slot
@@ -435,19 +458,50 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
     asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
 }
+// One test of the phase; a thread whose phase is not complete is suspended
+// until it completes or about a millisecond passes (the suspend-time hint),
+// instead of spinning on the test.
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     uint32_t ok;
     asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(1000000u)
         : "memory");
     return ok != 0;
 }
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
-    for (uint32_t it = 0; it < (1u << 22); it++)
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// bounded wait: false after limit_ns (about two seconds by default; at most
+// 2^22 tests)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint64_t limit_ns = 2000000000ull) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = global_ns();
+    for (uint32_t it = 0; it < (1u << 22); it++) {
         if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > limit_ns) return false;
+    }
     return false;
+}
+
+// Self-test of the bounded wait: one thread waits for a barrier phase that
+// nothing completes (no arrival, no copy); the wait must give up after
+// limit_ns and report it, and the context stays usable.  status[0] = 1 when
+// the wait gave up, status[1] = microseconds waited.
+__global__ void k_wait_selftest(uint32_t *status, uint64_t limit_ns) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        const uint64_t t0 = global_ns();
+        const bool done = mbar_wait_bounded(&bar, 0, limit_ns);
+        status[0] = done ? 0u : 1u;
+        const uint64_t us = (global_ns() - t0) / 1000u;
+        status[1] = us > 0xffffffffull ? 0xffffffffu : (uint32_t)us;
+    }
 }
 __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
@@ -598,7 +652,7 @@ __device__ __forceinline__ void zwrap_cell(const LatParams &p, const StepParams 
 }
 
 template <class S, int P, int COLL, int FEAT>
-__global__ void __launch_bounds__(BLOCK, sizeof(S) == 8 ? 2 : 3) k_bulk_tma(const __grid_constant__ LatParams p, const __grid_constant__ StepParams s) {
+__global__ void __launch_bounds__(Tma<S>::threads, Tma<S>::min_blocks) k_bulk_tma(const __grid_constant__ LatParams p, const __grid_constant__ StepParams s) {
     using R = typename Pop<S>::real;
     constexpr int NBUF = Nbuf<S>::value;
     constexpr uint32_t T = Tile<S>::cells, SLOT = slot_bytes<S>(), BUF = buf_bytes<S>();
@@ -614,7 +668,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(S) == 8 ? 2 : 3) k_bulk_tma(cons
     if (threadIdx.x == 0) {
         for (int q = 0; q < NBUF; q++) {
             mbar_init(&full[q], 1);
-            mbar_init(&empty[q], CTHREADS);
+            mbar_init(&empty[q], Tma<S>::cthreads);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -627,7 +681,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(S) == 8 ? 2 : 3) k_bulk_tma(cons
     }
     __syncthreads();
     S *pop = (S *)p.pop;
-    if (warp == CWARPS) {
+    if (warp == Tma<S>::cwarps) {
         // ------------------------------------------------ producer warp
         // iteration it (0 .. K+NBUF-1 for this block's K tiles): write back
         // tile it-NBUF from buffer it%NBUF once the compute warps released
@@ -696,7 +750,7 @@ __global__ void __launch_bounds__(BLOCK, sizeof(S) == 8 ? 2 : 3) k_bulk_tma(cons
         const uint32_t *fl = (const uint32_t *)(buf + 19 * SLOT);
         const uint32_t n0 = t * T;
 #pragma unroll 1
-        for (uint32_t c = threadIdx.x; c < T; c += CTHREADS) {
+        for (uint32_t c = threadIdx.x; c < T; c += Tma<S>::cthreads) {
             const uint32_t n = n0 + c;
             if (n >= p.N) break;
             const uint32_t fg = fl[c];
@@ -1057,7 +1111,7 @@ static unsigned tma_grid() {
         auto kern = k_bulk_tma<S, P, COLL, FEAT>;
         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem<S>());
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BLOCK, tma_smem<S>());
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, Tma<S>::threads, tma_smem<S>());
         g = (unsigned)(std::max(per_sm, 1) * num_sms());
     }
     return g;
@@ -1066,7 +1120,7 @@ static unsigned tma_grid() {
 template <class S, int P, int COLL, int FEAT>
 static void launch_tma(const LatParams &p, const StepParams &s, cudaStream_t st) {
     const unsigned ntiles = (unsigned)((p.N + Tile<S>::cells - 1) / Tile<S>::cells);
-    k_bulk_tma<S, P, COLL, FEAT><<<std::min(ntiles, tma_grid<S, P, COLL, FEAT>()), BLOCK, tma_smem<S>(), st>>>(p, s);
+    k_bulk_tma<S, P, COLL, FEAT><<<std::min(ntiles, tma_grid<S, P, COLL, FEAT>()), Tma<S>::threads, tma_smem<S>(), st>>>(p, s);
 }
 
 // one step: faces, wall cells (on the side stream `side` when they cannot
@@ -1196,6 +1250,11 @@ cudaError_t launch_sample(int storage, const LatParams &p, const StepParams &s, 
         case 3: sample_s<double>(p, s, q, verts, nvert, voff, vacc, sd, nslices, npix, sacc, st); break;
         default: return cudaErrorInvalidValue;
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wait_selftest(uint32_t *status, uint64_t limit_ns, cudaStream_t st) {
+    k_wait_selftest<<<1, 32, 0, st>>>(status, limit_ns);
     return cudaGetLastError();
 }
 

@@ -449,11 +449,11 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     // planes padded to 256 cells; a guard after the last plane covers the
     // shifted tile ranges the staged kernel fetches (largest offset NX*NY+NX+1)
     const uint64_t NP = (N + lbm::PLANE_ALIGN - 1) / lbm::PLANE_ALIGN * lbm::PLANE_ALIGN;
-    const uint64_t guard = (2048 + NX * NY + NX + 64 + lbm::PLANE_ALIGN - 1) / lbm::PLANE_ALIGN * lbm::PLANE_ALIGN;
+    const uint64_t guard = (lbm::TILE_MAX + NX * NY + NX + 64 + lbm::PLANE_ALIGN - 1) / lbm::PLANE_ALIGN * lbm::PLANE_ALIGN;
     h->pop_bytes = (19 * NP + guard) * sb;
     p.pop = h->dalloc(h->pop_bytes);
     p.NP = NP;
-    const uint64_t NFL = (N + 2047) / 2048 * 2048 + 2048;  // flags padded past the last tile (tiles up to 2048 cells)
+    const uint64_t NFL = (N + lbm::TILE_MAX - 1) / lbm::TILE_MAX * lbm::TILE_MAX + lbm::TILE_MAX;  // flags padded past the last tile
     p.flags = (uint32_t *)h->dalloc(NFL * 4);
     p.err = (uint32_t *)h->dalloc(16);
     p.recs = (uint32_t *)h->dalloc(nrec * lbm::RS * 4);
@@ -709,6 +709,27 @@ int lbm_get_kernel_times(lbm_lattice *h, lbm_kernel_times *out) {
             out->bulk_ms += c;
         }
     });
+}
+
+int lbm_selftest_copy_wait(uint64_t limit_ns, uint32_t *gave_up, uint64_t *waited_us) {
+    if (!gave_up || !waited_us || limit_ns == 0 || limit_ns > 10000000000ull) {
+        g_error = "lbm_selftest_copy_wait: null output or limit outside (0, 10 s]";
+        return LBM_ERR_INVALID;
+    }
+    uint32_t *d = nullptr;
+    uint32_t hst[2] = {0, 0};
+    cudaError_t e = cudaMalloc((void **)&d, sizeof(hst));
+    if (e == cudaSuccess) e = cudaMemset(d, 0, sizeof(hst));
+    if (e == cudaSuccess) e = lbm::launch_wait_selftest(d, limit_ns, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(hst, d, sizeof(hst), cudaMemcpyDeviceToHost);
+    if (d) cudaFree(d);
+    if (e != cudaSuccess) {
+        g_error = std::string("lbm_selftest_copy_wait: ") + cudaGetErrorString(e);
+        return LBM_ERR_CUDA;
+    }
+    *gave_up = hst[0];
+    *waited_us = hst[1];
+    return LBM_OK;
 }
 
 int lbm_set_timeout(lbm_lattice *h, double seconds) {

@@ -52,6 +52,7 @@ constexpr int BLOCK = 256;
 // flag bit of a fluid cell whose x neighbour is a planar x-face cell it feeds
 constexpr uint32_t FLAG_XFACE = 0x80000000u;
 constexpr uint32_t PLANE_ALIGN = 256;  // cells
+constexpr uint32_t TILE_MAX = 4096;    // cells of the staged kernel's largest tile (allocation guards)
 
 // error bits set by kernels (read by the host after each chunk)
 constexpr uint32_t ERR_COPY_WAIT = 1u;  // a bulk-copy wait passed its iteration limit

@@ -179,6 +179,7 @@ def library() -> C.CDLL:
     L.lbm_stream.argtypes = [vp, C.POINTER(vp)]
     L.lbm_synchronize.argtypes = [vp]
     L.lbm_set_timeout.argtypes = [vp, C.c_double]
+    L.lbm_selftest_copy_wait.argtypes = [u64, C.POINTER(C.c_uint32), C.POINTER(u64)]
     L.lbm_profile.argtypes = [vp, i32]
     L.lbm_get_kernel_times.argtypes = [vp, C.POINTER(_KernelTimes)]
     L.lbm_macros.argtypes = [vp, C.POINTER(C.c_float)]
@@ -655,6 +656,18 @@ def record_forces_noalloc(records_dev_ptr: int, nrec: int, forces_dev_ptr: int, 
         buf = C.create_string_buffer(512)
         L.lbm_noalloc_error(buf, 512)
         raise LbmError(rc, buf.value.decode(errors="replace"))
+
+
+def selftest_copy_wait(limit_s: float = 0.005) -> tuple[bool, float]:
+    """Runs the step kernel's bounded wait on a copy barrier that nothing
+    completes, limited to `limit_s` seconds: returns (gave_up, seconds waited).
+    The wait ends by itself; no fault and no hang."""
+    gave_up = C.c_uint32(0)
+    waited = C.c_uint64(0)
+    rc = library().lbm_selftest_copy_wait(int(limit_s * 1e9), C.byref(gave_up), C.byref(waited))
+    if rc != 0:
+        raise _global_error(rc)
+    return bool(gave_up.value), waited.value * 1e-6
 
 
 def halfway(vox: StaticVoxels) -> StaticVoxels:

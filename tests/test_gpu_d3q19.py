@@ -141,6 +141,21 @@ def test_periodic_z_with_open_sides(storage):
     assert abs(hg[-1, 0] / ho[-1, 0] - 1.0) < max(10 * tol, 1e-5)
 
 
+def test_bounded_copy_wait_gives_up_and_device_stays_usable():
+    """The step kernel's barrier waits end by themselves: a wait on a phase
+    nothing completes gives up at its limit (5 ms here) and reports it; a
+    lattice then still steps normally."""
+    from simlab_b200.lbm import selftest_copy_wait
+
+    gave_up, waited = selftest_copy_wait(0.005)
+    assert gave_up
+    assert 0.005 <= waited < 0.5
+    st, vox = feature_case(Storage.FP16)
+    g = Lattice(st, vox)
+    f = g.run(4)
+    assert np.isfinite(f).all()
+
+
 def test_checkpoint_round_trip_is_exact():
     st, vox = feature_case(Storage.FP16)
     g = Lattice(st, vox)
