@@ -104,9 +104,10 @@ __device__ R wall_tau(const LatParams &p, const Consts<R> &k, uint32_t r, uint32
 //
 // SC is the storage scale: f holds SC * (f_i - w_i) on entry and receives the
 // post-collision values in the same units (SC = 32768 for FP16 storage, 1
-// otherwise).  Scaling by a power of two is exact, so the moments equal those
-// of the unscaled populations bit for bit, and the scale of the outputs rides
-// on compile-time weights.
+// otherwise).  Scaling by a power of two is exact, so the collision can work
+// on the scaled moments (rescaling only the density and 1/rho) and give the
+// unscaled results times the scale bit for bit; the scale of the outputs
+// rides on compile-time weights.
 //
 // The 9 opposite pairs (i = 2k+1, o = 2k+2) share c c, so the equilibrium,
 // the non-equilibrium projection, the absorbing target and the forcing term
@@ -117,33 +118,36 @@ __device__ R wall_tau(const LatParams &p, const Consts<R> &k, uint32_t r, uint32
 // FEAT selects compile-time feature sets for the hot loop: 0 reads every
 // switch from the parameters; odd values fix forcing and the u_inf absorbing
 // target off and LES to bit 1.
+//
+// relax_m takes the moments m of f already computed (the regularized
+// collision reads f only through them; plain BGK also reads f itself).
 template <class R, int COLL, int SC = 1, int FEAT = 0>
-__device__ __forceinline__ void relax(const LatParams &p, const Consts<R> &k, R *f, uint32_t x, uint32_t y, uint32_t z,
-                                      bool wall, uint32_t r, uint32_t mask, R pcx, R pcy, R pcz, const R *om, R &rho_o, R &ux_o,
-                                      R &uy_o, R &uz_o) {
+__device__ __forceinline__ void relax_m(const LatParams &p, const Consts<R> &k, const Moments<R> &m, R *f, uint32_t x, uint32_t y,
+                                        uint32_t z, bool wall, uint32_t r, uint32_t mask, R pcx, R pcy, R pcz, const R *om, R &rho_o,
+                                        R &ux_o, R &uy_o, R &uz_o) {
     constexpr bool SPEC = (FEAT & 1) != 0;
     const bool les_on = SPEC ? (FEAT & 2) != 0 : (p.les_on != 0);
     const bool forcing = SPEC ? false : (p.forcing != 0);
     const bool abs_u = SPEC ? false : (p.abs_u != 0);
+    // the moments stay in storage units; only rho1 and 1/rho are rescaled,
+    // and the non-equilibrium stress pi (in storage units as well) meets
+    // weights without the scale
     const R isc = (R)(1.0 / SC);
-    Moments<R> m = moments<R>(f);
-    if (SC != 1) {
-        m.rho1 *= isc; m.jx *= isc; m.jy *= isc; m.jz *= isc;
-        m.sxx *= isc; m.syy *= isc; m.szz *= isc; m.sxy *= isc; m.sxz *= isc; m.syz *= isc;
-    }
-    const R rho = (R)1 + m.rho1;
+    const R rho1 = SC != 1 ? m.rho1 * isc : m.rho1;
+    const R rho = (R)1 + rho1;
     const R irho = (R)1 / rho;
-    const R ux = m.jx * irho + (R)0.5 * k.grav[0];
-    const R uy = m.jy * irho + (R)0.5 * k.grav[1];
-    const R uz = m.jz * irho + (R)0.5 * k.grav[2];
+    const R irs = SC != 1 ? irho * isc : irho;
+    const R ux = m.jx * irs + (R)0.5 * k.grav[0];
+    const R uy = m.jy * irs + (R)0.5 * k.grav[1];
+    const R uz = m.jz * irs + (R)0.5 * k.grav[2];
     R pi[6];
-    pi_neq<R>(m, rho, ux, uy, uz, pi);
+    pi_neq<R>(m, SC != 1 ? rho * (R)SC : rho, ux, uy, uz, pi);
     R tau = k.tau0;
     if (les_on) {
         // Smagorinsky tau from |Pi_neq| (shader.rs:825-828)
         const R pp = pi[0] * pi[0] + pi[1] * pi[1] + pi[2] * pi[2] + (R)2 * (pi[3] * pi[3] + pi[4] * pi[4] + pi[5] * pi[5]);
         const R qn = sqrt((R)2 * pp);
-        tau = (R)0.5 * (k.tau0 + sqrt(k.tau0 * k.tau0 + (R)18 * k.smag2 * qn * irho));
+        tau = (R)0.5 * (k.tau0 + sqrt(k.tau0 * k.tau0 + (R)18 * k.smag2 * qn * irs));
     }
     if (wall && p.wall_model && mask != 0u) tau = wall_tau<R>(p, k, r, mask, pcx, pcy, pcz, ux, uy, uz, tau, om);
     R sp = 0;
@@ -171,7 +175,7 @@ __device__ __forceinline__ void relax(const LatParams &p, const Consts<R> &k, R 
     //   regularized: v = fe + (1 - omega) fneq + delta
     //   BGK:         v = (1 - omega) f + omega fe + delta
     const R wa = (R)(SC / 18.0), we = (R)(SC / 36.0), w0 = (R)(SC / 3.0);
-    const R Bq = m.rho1 - rho * usq;
+    const R Bq = rho1 - rho * usq;
     const R lam = COLL == 1 ? omg : (R)1;
     R cA, cB, cO, dB;  // coefficient multipliers (unit weight) and the constant shift
     if (abs_u) {
@@ -181,7 +185,7 @@ __device__ __forceinline__ void relax(const LatParams &p, const Consts<R> &k, R 
         cO = l2 * (R)3 * rho;
         dB = 0;
     } else {
-        const R sr = sg * m.rho1;
+        const R sr = sg * rho1;
         cA = (R)4.5 * (lam * rho - sr);
         cB = lam * Bq;
         dB = -sr * ((R)1 - usq);
@@ -189,7 +193,8 @@ __device__ __forceinline__ void relax(const LatParams &p, const Consts<R> &k, R 
     }
     const R sgsc = sg * (R)SC;  // for the u_inf target, in storage units
     const R A_a = wa * cA, A_e = we * cA, B_a = wa * (cB + dB), B_e = we * (cB + dB), O_a = wa * cO, O_e = we * cO;
-    const R Cn_a = (R)4.5 * wa * om1, Cn_e = (R)4.5 * we * om1;
+    // pi is in storage units: its weights carry no scale
+    const R Cn_a = SC != 1 ? (R)(4.5 / 18.0) * om1 : (R)4.5 * wa * om1, Cn_e = SC != 1 ? (R)(4.5 / 36.0) * om1 : (R)4.5 * we * om1;
     // c c : Pi - tr for edges = (Pi_aa - tr/2) + (Pi_bb - tr/2) + 2 s Pi_ab
     const R ht = (R)0.5 * tr;
     const R qx = pi[0] - ht, qy = pi[1] - ht, qz = pi[2] - ht;
@@ -197,7 +202,7 @@ __device__ __forceinline__ void relax(const LatParams &p, const Consts<R> &k, R 
     {
         R v = w0 * (cB + dB);
         if (COLL == 1) v = v + om1 * f[0];
-        else v = v - ((R)4.5 * w0 * om1) * tr;
+        else v = v - (SC != 1 ? (R)(4.5 / 3.0) * om1 : (R)4.5 * w0 * om1) * tr;
         if (abs_u) v = v + sgsc * k.ft_rest;
         if (forcing) v = v + w0 * (fo * ((R)-3 * uG));
         f[0] = v;
@@ -248,6 +253,13 @@ __device__ __forceinline__ void relax(const LatParams &p, const Consts<R> &k, R 
     }
     rho_o = rho; ux_o = ux; uy_o = uy; uz_o = uz;
 }
+template <class R, int COLL, int SC = 1, int FEAT = 0>
+__device__ __forceinline__ void relax(const LatParams &p, const Consts<R> &k, R *f, uint32_t x, uint32_t y, uint32_t z,
+                                      bool wall, uint32_t r, uint32_t mask, R pcx, R pcy, R pcz, const R *om, R &rho_o, R &ux_o,
+                                      R &uy_o, R &uz_o) {
+    relax_m<R, COLL, SC, FEAT>(p, k, moments<R>(f), f, x, y, z, wall, r, mask, pcx, pcy, pcz, om, rho_o, ux_o, uy_o, uz_o);
+}
+
 
 // ---------------------------------------------------------------- bulk
 // Plain fluid cells (flag word 0): the hot loop.
@@ -387,20 +399,25 @@ __global__ void __launch_bounds__(BLOCK) k_faces(const __grid_constant__ LatPara
 // flight while the current one is collided).  Every mbarrier wait is
 // bounded; on expiry the block records ERR_COPY_WAIT, drains its copies
 // (bounded) and stops.
-// Warp-specialized: the first Tma<S>::cwarps warps collide, the last warp is
-// the producer that issues the bulk loads and stores.  Per buffer a "full"
-// mbarrier (producer arrival + transaction bytes) and an "empty" mbarrier
-// (one arrival per compute thread) replace block barriers, so compute warps
-// move on to the next tile while the producer writes the last one back.
-// Block shape per storage: compute warps, cells per compute thread and tile,
-// tile buffers, and the blocks per SM the register budget aims at.  Measured
-// on the B200 with the 512x256x256 arm case (MLUPS FP16 / FP32): three blocks
-// of 7 compute warps with 896- / 448-cell tiles 54.9 / 35.3 k; two blocks of
-// 10 warps, 1280 / 640 cells 52.3 / 35.5 k; one block of 20 warps with three
-// buffers of 1280 / 640 cells 46.3 / 34.6 k; one block of 20 warps with two
-// buffers of 2560 / 1280 cells 55.7 / 38.1 k.  The copy engine takes a few
-// hundred cycles per bulk copy (one per plane and tile, each way), so the
-// fewer and larger the copies per SM, the sooner a buffer turns around.
+// Warp-specialized: the first Tma<S>::cwarps warps collide, the last
+// Tma<S>::pwarps warps are producers that issue the bulk loads and stores
+// (producer p handles the planes j = p mod pwarps).  Per buffer a "full"
+// mbarrier (one arrival per producer + transaction bytes) and an "empty"
+// mbarrier (one arrival per compute thread) replace block barriers, so
+// compute warps move on to the next tile while the producers write the last
+// one back.
+// Block shape per storage: compute warps, producer warps, cells per compute
+// thread and tile, tile buffers, and the blocks per SM the register budget
+// aims at.  Measured on the B200 with the 512x256x256 arm case (MLUPS FP16 /
+// FP32): three blocks of 7 compute warps with 896- / 448-cell tiles 54.9 /
+// 35.3 k; two blocks of 10 warps, 1280 / 640 cells 52.3 / 35.5 k; one block of
+// 20 warps with three buffers of 1280 / 640 cells 46.3 / 34.6 k; one block of
+// 20 warps with two buffers of 2560 / 1280 cells 56.4 / 38.9 k; the same with
+// 2, 3, 4, 5 producer warps 59.8, 60.3, 60.5, 58.7 k FP16 (FP32 38.2 k with 2 or
+// 3).  The copy engine takes a few hundred cycles per bulk copy (one per plane
+// and tile, each way) and the copies one warp issues go one after another, so
+// fewer, larger copies and several issuing warps shorten a buffer's
+// turnaround.
 #ifndef LBM_CWARPS_2B
 #define LBM_CWARPS_2B 20  // compute warps per block for 2-byte storage
 #endif
@@ -412,6 +429,12 @@ __global__ void __launch_bounds__(BLOCK) k_faces(const __grid_constant__ LatPara
 #endif
 #ifndef LBM_BLOCKS_2B
 #define LBM_BLOCKS_2B 1  // blocks per SM for 2-byte storage
+#endif
+#ifndef LBM_PWARPS_2B
+#define LBM_PWARPS_2B 4  // producer warps per block for 2-byte storage
+#endif
+#ifndef LBM_PWARPS_4B
+#define LBM_PWARPS_4B 1
 #endif
 #ifndef LBM_CWARPS_4B
 #define LBM_CWARPS_4B 20  // the same for 4-byte storage
@@ -427,7 +450,8 @@ __global__ void __launch_bounds__(BLOCK) k_faces(const __grid_constant__ LatPara
 #endif
 template <class S> struct Tma {
     static constexpr int cwarps = sizeof(S) == 2 ? LBM_CWARPS_2B : (sizeof(S) == 4 ? LBM_CWARPS_4B : 7);
-    static constexpr int cthreads = cwarps * 32, threads = cthreads + 32;  // + the producer warp
+    static constexpr int pwarps = sizeof(S) == 2 ? LBM_PWARPS_2B : (sizeof(S) == 4 ? LBM_PWARPS_4B : 1);
+    static constexpr int cthreads = cwarps * 32, threads = cthreads + 32 * pwarps;  // + the producer warps
     static constexpr uint32_t cells = (uint32_t)(sizeof(S) == 2 ? LBM_TILE_2B : (sizeof(S) == 4 ? LBM_TILE_4B : 1)) * cthreads;
     static constexpr int nbuf = sizeof(S) == 2 ? LBM_NBUF_2B : (sizeof(S) == 4 ? LBM_NBUF_4B : 3);
     static constexpr int min_blocks = sizeof(S) == 2 ? LBM_BLOCKS_2B : (sizeof(S) == 4 ? LBM_BLOCKS_4B : 2);
@@ -522,19 +546,24 @@ __device__ __forceinline__ int64_t plane_shift(int j, int64_t NX, int64_t NXY) {
     return (P == 0 || j == 0) ? 0 : (int64_t)CX(j) + (int64_t)CY(j) * NX + (int64_t)CZ(j) * NXY;
 }
 
-template <class S, int P>
-__device__ __forceinline__ void tma_load_tile(const LatParams &p, uint8_t *buf, uint64_t *bar, uint32_t n0) {
+// The loads of tile n0 into a buffer by producer warp pw of NPROD: the
+// planes j = pw (mod NPROD), and the flags from the last producer; each
+// producer posts its own bytes on the buffer's "full" barrier.
+template <class S, int P, int NPROD>
+__device__ __forceinline__ void tma_load_tile(const LatParams &p, uint8_t *buf, uint64_t *bar, uint32_t n0, int pw) {
     constexpr uint32_t SLOT = slot_bytes<S>();
     constexpr uint32_t T = Tile<S>::cells;
     const S *pop = (const S *)p.pop;
     const int64_t NX = p.NX, NXY = (int64_t)p.NX * p.NY;
-    mbar_expect_tx(bar, 19 * SLOT + T * 4);
+    const uint32_t nplanes = (uint32_t)((19 - pw + NPROD - 1) / NPROD);
+    mbar_expect_tx(bar, nplanes * SLOT + (pw == NPROD - 1 ? T * 4 : 0u));
 #pragma unroll
     for (int j = 0; j < 19; j++) {
+        if (j % NPROD != pw) continue;
         const int64_t e = (int64_t)j * (int64_t)p.NP + n0 + plane_shift<P>(j, NX, NXY) - lead<S, P>(j);
         bulk_g2s(buf + j * SLOT, pop + e, SLOT, bar);
     }
-    bulk_g2s(buf + 19 * SLOT, p.flags + n0, T * 4, bar);
+    if (pw == NPROD - 1) bulk_g2s(buf + 19 * SLOT, p.flags + n0, T * 4, bar);
 }
 
 // The x-face cell b next to cell m (b = m - 1 when x = 1, b = m + 1 when
@@ -667,7 +696,7 @@ __global__ void __launch_bounds__(Tma<S>::threads, Tma<S>::min_blocks) k_bulk_tm
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
         for (int q = 0; q < NBUF; q++) {
-            mbar_init(&full[q], 1);
+            mbar_init(&full[q], Tma<S>::pwarps);
             mbar_init(&empty[q], Tma<S>::cthreads);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -681,11 +710,14 @@ __global__ void __launch_bounds__(Tma<S>::threads, Tma<S>::min_blocks) k_bulk_tm
     }
     __syncthreads();
     S *pop = (S *)p.pop;
-    if (warp == Tma<S>::cwarps) {
-        // ------------------------------------------------ producer warp
+    if (warp >= Tma<S>::cwarps) {
+        constexpr int NPROD = Tma<S>::pwarps;
+        const int pw = warp - Tma<S>::cwarps;  // this producer's planes: j = pw (mod NPROD)
+        // ------------------------------------------------ producer warps
         // iteration it (0 .. K+NBUF-1 for this block's K tiles): write back
-        // tile it-NBUF from buffer it%NBUF once the compute warps released
-        // it, then load tile it into the same buffer
+        // this producer's planes of tile it-NBUF from buffer it%NBUF once the
+        // compute warps released it, then load them for tile it into the
+        // same buffer (the producers' planes are disjoint slots)
         const int64_t N = p.N;
         const uint32_t G = gridDim.x;
         const uint32_t K = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / G + 1 : 0;
@@ -695,11 +727,11 @@ __global__ void __launch_bounds__(Tma<S>::threads, Tma<S>::min_blocks) k_bulk_tm
             const int b = it % NBUF;
             if (it >= NBUF) {
                 if (!mbar_wait_bounded(&empty[b], ((it - NBUF) / NBUF) & 1)) { alive = false; break; }
-                if (lane < 19) {
+                if (pw + NPROD * lane < 19) {
                     // plane j's slots of the tile's cells back to HBM: cells
                     // and slots clamped to [0, N); the 16-byte-aligned interior
                     // with one bulk store, the ragged ends with plain stores
-                    const int j = lane;
+                    const int j = pw + NPROD * lane;
                     const uint32_t n0 = (blockIdx.x + (it - NBUF) * G) * T;
                     const int64_t sh = tab_sh[j];
                     const int64_t lo = max((int64_t)n0, -sh);
@@ -720,7 +752,7 @@ __global__ void __launch_bounds__(Tma<S>::threads, Tma<S>::min_blocks) k_bulk_tm
             }
             if (it < K && lane == 0) {
                 fence_async_smem();
-                tma_load_tile<S, P>(p, sm + b * BUF, &full[b], (blockIdx.x + it * G) * T);
+                tma_load_tile<S, P, NPROD>(p, sm + b * BUF, &full[b], (blockIdx.x + it * G) * T, pw);
             }
         }
         if (!alive && lane == 0) {
@@ -733,7 +765,7 @@ __global__ void __launch_bounds__(Tma<S>::threads, Tma<S>::min_blocks) k_bulk_tm
                 if (last >= 0) mbar_wait_bounded(&full[bq], ((uint32_t)last / NBUF) & 1);
             }
         }
-        if (lane < 19) bulk_wait_all();
+        if (pw + NPROD * lane < 19) bulk_wait_all();
         return;
     }
     // ---------------------------------------------------- compute warps

@@ -419,12 +419,9 @@ struct Moments {
 // shader.rs:341-365, from the sums s_k and differences d_k of the 9
 // opposite pairs (2k+1, 2k+2)
 template <class R>
-__device__ __forceinline__ Moments<R> moments(const R *f) {
-    R s[9], d[9];
-#pragma unroll
-    for (int k = 0; k < 9; k++) { s[k] = f[2 * k + 1] + f[2 * k + 2]; d[k] = f[2 * k + 1] - f[2 * k + 2]; }
+__device__ __forceinline__ Moments<R> moments_sd(R f0, const R *s, const R *d) {
     Moments<R> m;
-    m.rho1 = f[0] + ((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7])) + s[8];
+    m.rho1 = f0 + ((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7])) + s[8];
     // odd members: 1 (1,0,0) 3 (0,1,0) 5 (0,0,1) 7 (1,1,0) 9 (1,0,1) 11 (0,1,1) 13 (1,-1,0) 15 (1,0,-1) 17 (0,1,-1)
     m.jx = (d[0] + d[3]) + (d[4] + d[6]) + d[7];
     m.jy = (d[1] + d[3]) + (d[5] - d[6]) + d[8];
@@ -436,6 +433,13 @@ __device__ __forceinline__ Moments<R> moments(const R *f) {
     m.sxz = s[4] - s[7];
     m.syz = s[5] - s[8];
     return m;
+}
+template <class R>
+__device__ __forceinline__ Moments<R> moments(const R *f) {
+    R s[9], d[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) { s[k] = f[2 * k + 1] + f[2 * k + 2]; d[k] = f[2 * k + 1] - f[2 * k + 2]; }
+    return moments_sd<R>(f[0], s, d);
 }
 
 // shader.rs:818-824: non-equilibrium stress from shifted moments
