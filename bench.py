@@ -293,6 +293,89 @@ def d3q27_levels():
     return res
 
 
+def c5_throughput(steps: int = 40, warmup: int = 4):
+    """The at-scale throughput case: D3Q19 LES with FP16 populations on a
+    1024x512x512 lattice (268,435,456 cells) around the arm scaled x2, MLUPS
+    of the step and the bulk kernel's fraction of the measured copy
+    bandwidth (80 B per cell)."""
+    import torch
+
+    from simlab_b200.cases import arm_les
+    from simlab_b200.lbm import Lattice, Storage
+
+    st, vox = arm_les(Storage.FP16, scale=2)
+    lat = Lattice(st, vox)
+    stream = torch.cuda.ExternalStream(lat.stream)
+    lat.advance(warmup)
+    lat.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record()
+    lat.advance(steps)
+    with torch.cuda.stream(stream):
+        e1.record()
+    lat.synchronize()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    lat.profile(True)  # the bulk kernel's own time, events around it on the next steps
+    lat.advance(10)
+    lat.synchronize()
+    kt = lat.kernel_times()
+    lat.profile(False)
+    mass, bad = lat.mass()
+    cells = st.cells()
+    bulk_ms = kt["bulk_ms"] / max(kt["steps"], 1)
+    hbm, _ = peaks()
+    res = {"dims": list(st.dims), "cells": cells, "mlups": round(cells * steps / ms / 1e3, 1), "ms_per_step": round(ms / steps, 4),
+           "bulk_ms": round(bulk_ms, 4), "bulk_hbm_frac": round(80.0 * cells / (bulk_ms * 1e-3) / 1e9 / hbm, 4),
+           "nonfinite": int(bad), "memory_gb": round(lat.info().memory_bytes / 1e9, 2)}
+    lat.close()
+    return res
+
+
+def c5_adjoint():
+    """The at-scale adjoint (simlab_b200.cases.prop_gray_band): the rotor held
+    still as a gray body on one 384x192x192 D3Q19 level, gradient of the mean
+    torque over steps 301-600 with respect to the 3-cell band around it.
+    FP16-stored forward with the FP32 adjoint, moments kept where they fit in
+    device memory and the rest recomputed from checkpoints; the FP32-stored
+    run alongside for the gradient's agreement."""
+    import torch
+
+    from simlab_b200.cases import prop_gray_band
+    from simlab_b200.gray import GrayLattice
+    from simlab_b200.lbm import Storage
+
+    out = {"workload": "rotor R60 as a gray body, 384x192x192, torque over steps 301-600, 3-cell design band, checkpoint every 50"}
+    grads = {}
+    for storage in (Storage.FP16, Storage.FP32):
+        st, gam, band, spec = prop_gray_band(storage)
+        lat = GrayLattice(st, gam)
+        stream = torch.cuda.ExternalStream(lat.stream)
+        lat.run(20)
+        lat.reset()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record()
+        lat.run(spec.steps)
+        with torch.cuda.stream(stream):
+            e1.record()
+        torch.cuda.synchronize()
+        fwd = e0.elapsed_time(e1)
+        J, g = lat.backward(spec)
+        t = lat.backward_times()
+        tot = t["forward_ms"] + t["recompute_ms"] + t["reverse_ms"]
+        grads[storage] = g[band]
+        out[storage.name.lower()] = {"forward_solve_ms": round(fwd, 3), "forward_mlups": round(st.cells() * spec.steps / fwd / 1e3, 1),
+                                     "backward_ms": round(tot, 3), "ratio": round(tot / fwd, 3), "torque": J, "band_cells": int(band.sum()),
+                                     "first_pass_ms": round(t["forward_ms"], 3), "recompute_ms": round(t["recompute_ms"], 3),
+                                     "reverse_ms": round(t["reverse_ms"], 3)}
+        lat.close()
+    a, b = grads[Storage.FP16], grads[Storage.FP32]
+    out["fp16_vs_fp32_grad_rel_l2"] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+    return out
+
+
 def run_reference(args, ws, rank):
     if rank != 0:
         return
@@ -409,6 +492,8 @@ def main():
     if ws == 1 and not args.no_extras:
         line["adjoint"] = adjoint_ratio()
         line["d3q27_three_levels_mlups"] = d3q27_levels()
+        line["c5_fp16_1024x512x512"] = c5_throughput()
+        line["c5_adjoint"] = c5_adjoint()
     if rank == 0 and ws == 1 and not args.no_cpu:
         v, cores, sample = cpu_sample(Storage.FP16)
         line["cpu_baseline"] = {"value": round(v, 3), "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}

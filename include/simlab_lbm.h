@@ -400,7 +400,8 @@ typedef struct {
     uint32_t dims[3];
     uint32_t box_lo[3];         /* design box: first cell and size per axis */
     uint32_t box_n[3];
-    int32_t storage;            /* LBM_STORAGE_FP32 or LBM_STORAGE_FP64 */
+    int32_t storage;            /* LBM_STORAGE_FP32, _FP64, or _FP16 (populations stored as FP16, arithmetic,
+                                   moments and adjoint FP32) */
     double nu;                  /* lattice viscosity, tau = 0.5 + 3 nu */
     double u_in[3];             /* inlet velocity (and initial state) */
     double alpha;               /* momentum fraction removed per step at gamma = 1 (0 < alpha <= 1) */

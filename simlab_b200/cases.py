@@ -186,3 +186,37 @@ def prop_refined(storage=Storage.FP32, radius=60.0, tip_speed=0.08, u=0.02, nu_f
     ax_lo, ax_hi = int(np.floor(c[0] + sv.axial[0])) - 3, int(np.ceil(c[0] + sv.axial[1])) + 3
     geo = SpinGeometry(vox=sv, box_lo=[ax_lo, int(c[1]) - r, int(c[2]) - r], box_n=[ax_hi - ax_lo + 1, 2 * r + 2, 2 * r + 2])
     return s, geo, tip_speed / radius
+
+
+# ------------------------------------------------------------------ at-scale adjoint case
+def prop_gray_band(storage=Storage.FP16, dims=(384, 192, 192), radius=60.0, band=3.0, u=0.04, nu=0.02, steps=600, checkpoint_every=50):
+    """The at-scale adjoint case: the two-blade rotor of the refined case
+    (radius 60 cells, axis along the flow) held still on one 384x192x192
+    D3Q19 level as a gray body: its cells at solid fraction 1, the fluid cells
+    within `band` cells of it design cells at 0.5; the objective is the mean
+    torque about the rotor axis over the second half of `steps`, with the
+    moments kept where they fit in device memory and the other segments
+    recomputed from checkpoints every `checkpoint_every` steps.  Returns the
+    setup, gamma (design-box order, x fastest), the band mask in that order
+    and the adjoint spec."""
+    from .gray import AdjointSpec, GraySetup
+    from .lbm import inside_grid
+    from .shapes import propeller
+    from scipy.ndimage import distance_transform_edt
+
+    c = np.array([0.5 * (dims[0] - 1) - 64.0 + 0.31, 0.5 * (dims[1] - 1) + 0.23, 0.5 * (dims[2] - 1) + 0.17])
+    v, t = propeller(radius=radius)
+    vl = np.asarray(v, dtype=np.float64) @ BODY_TO_LATTICE.T + c
+    m = int(np.ceil(band)) + 2
+    lo = np.maximum(np.floor(vl.min(axis=0)).astype(int) - m, 1)
+    hi = np.minimum(np.ceil(vl.max(axis=0)).astype(int) + m, np.array(dims) - 2)
+    n = hi - lo + 1
+    solid = inside_grid(vl, t, lo.astype(float), 1.0, n).reshape(n[2], n[1], n[0])
+    dist = distance_transform_edt(~solid)
+    near = (~solid) & (dist <= band)
+    gam = np.where(solid, 1.0, np.where(near, 0.5, 0.0)).reshape(-1)
+    st = GraySetup(dims=list(dims), box_lo=[int(x) for x in lo], box_n=[int(x) for x in n], nu=nu, u_in=[u, 0.0, 0.0], alpha=1.0,
+                   center=[float(x) for x in c], storage=storage)
+    spec = AdjointSpec(steps=steps, t0=steps // 2 + 1, t1=steps, checkpoint_every=checkpoint_every, objective=1, dir=[1.0, 0.0, 0.0],
+                       recompute=False)
+    return st, gam, near.reshape(-1), spec

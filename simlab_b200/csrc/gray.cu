@@ -31,6 +31,10 @@
 //
 // Traffic per cell update (FP32): forward 152 B (19 loads + 19 stores) + 4 B
 // of a; moments 16 B more when kept; adjoint 152 B + 16 B of moments + 4 B.
+// FP16 storage halves the forward's population traffic and the checkpoints;
+// the moments, the adjoint and the arithmetic stay FP32 (the rounding is not
+// differentiated: the gradient is the adjoint of the FP32 update along the
+// stored trajectory).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -158,35 +162,53 @@ __device__ __forceinline__ void block_reduce6(double *v, double *partials, uint3
     if (threadIdx.x == 0) *ticket = 0u;
 }
 
-template <class R>
-__global__ void __launch_bounds__(BLK) kg_init(const __grid_constant__ GParams p, R *P) {
+// Storage S of the populations: float, double, or __half (FP32 arithmetic,
+// f - w scaled by 32768 and rounded stochastically, as the engine stores
+// FP16); rn() rounds a constant to nearest (inlet and initial values).
+template <class S> struct GS {
+    using R = typename lbm::Pop<S>::real;
+    static __device__ __forceinline__ S rn(R v) { return (S)v; }
+};
+template <> struct GS<__half> {
+    using R = float;
+    static __device__ __forceinline__ __half rn(float v) { return __float2half_rn(v * 32768.0f); }
+};
+
+template <class S>
+__global__ void __launch_bounds__(BLK) kg_init(const __grid_constant__ GParams p, S *P) {
+    using R = typename GS<S>::R;
     const uint32_t n = blockIdx.x * BLK + threadIdx.x;
     if (n >= p.N) return;
     const GConsts<R> &k = KG<R>(p);
 #pragma unroll
-    for (int i = 0; i < 19; i++) P[(uint64_t)i * p.NP + n] = k.feq_in[i];
+    for (int i = 0; i < 19; i++) P[(uint64_t)i * p.NP + n] = GS<S>::rn(k.feq_in[i]);
 }
 
 // x = 0: inlet equilibrium; x = NX-1: copy of x = NX-2
-template <class R>
-__global__ void __launch_bounds__(BLK) kg_faces(const __grid_constant__ GParams p, R *P) {
+template <class S>
+__global__ void __launch_bounds__(BLK) kg_faces(const __grid_constant__ GParams p, S *P) {
+    using R = typename GS<S>::R;
     const uint32_t r = blockIdx.x * BLK + threadIdx.x;  // row (y, z)
     if (r >= p.NY * p.NZ) return;
     const GConsts<R> &k = KG<R>(p);
     const uint32_t b0 = r * p.NX, b1 = b0 + p.NX - 1;
 #pragma unroll
     for (int i = 0; i < 19; i++) {
-        P[(uint64_t)i * p.NP + b0] = k.feq_in[i];
+        P[(uint64_t)i * p.NP + b0] = GS<S>::rn(k.feq_in[i]);
         P[(uint64_t)i * p.NP + b1] = P[(uint64_t)i * p.NP + b1 - 1];
     }
 }
 
 // one step of the bulk (1 <= x <= NX-2).  MOM: (rho - 1, j) of every cell's
 // pre-collision state into 4 planes of NP; FORCE: a * j of every design-box
-// cell into 3 planes of the box (summed by kg_force)
-template <class R, bool MOM, bool FORCE>
-__global__ void __launch_bounds__(BLK) kg_step(const __grid_constant__ GParams p, const R *__restrict__ src, R *__restrict__ dst,
-                                               R *__restrict__ mom, R *__restrict__ fbox) {
+// cell into 3 planes of the box (summed by kg_force).  FP16 storage rounds
+// stochastically from a hash of the cell and the step (seed_mix), so a
+// segment recomputed from its checkpoint repeats the first pass bit for bit.
+template <class S, bool MOM, bool FORCE>
+__global__ void __launch_bounds__(BLK) kg_step(const __grid_constant__ GParams p, const S *__restrict__ src, S *__restrict__ dst,
+                                               typename GS<S>::R *__restrict__ mom, typename GS<S>::R *__restrict__ fbox,
+                                               uint32_t seed_mix) {
+    using R = typename GS<S>::R;
     const uint32_t n = blockIdx.x * BLK + threadIdx.x;
     if (n >= p.N) return;
     uint32_t x, y, z;
@@ -196,7 +218,7 @@ __global__ void __launch_bounds__(BLK) kg_step(const __grid_constant__ GParams p
     const Off o = make_off(p, y, z);
     R g[19];
 #pragma unroll
-    for (int i = 0; i < 19; i++) g[i] = src[(uint64_t)i * p.NP + (uint32_t)((int32_t)n + o.at(-CX(i), -CY(i), -CZ(i)))];
+    for (int i = 0; i < 19; i++) g[i] = lbm::Pop<S>::cvt(src[(uint64_t)i * p.NP + (uint32_t)((int32_t)n + o.at(-CX(i), -CY(i), -CZ(i)))]);
     R rho1 = 0, j[3] = {0, 0, 0};
 #pragma unroll
     for (int i = 0; i < 19; i++) {
@@ -210,11 +232,12 @@ __global__ void __launch_bounds__(BLK) kg_step(const __grid_constant__ GParams p
     const R jj = j[0] * j[0] + j[1] * j[1] + j[2] * j[2];
     const R B = w - (R)1 + ((R)1 - an) * ((R)1 - an);
     const R c1 = (R)3 * (w - an), bq = B * irho;
+    lbm::Rng rng{lbm::sr_hash_mix(n, seed_mix)};
 #pragma unroll
     for (int i = 0; i < 19; i++) {
         const R cj = (R)CX(i) * j[0] + (R)CY(i) * j[1] + (R)CZ(i) * j[2];
         const R Q = (R)4.5 * cj * cj - (R)1.5 * jj;
-        dst[(uint64_t)i * p.NP + n] = ((R)1 - w) * g[i] + (R)WD(i) * (w * rho1 + c1 * cj + bq * Q);
+        dst[(uint64_t)i * p.NP + n] = lbm::Pop<S>::enc(((R)1 - w) * g[i] + (R)WD(i) * (w * rho1 + c1 * cj + bq * Q), rng);
     }
     if (MOM) {
         mom[n] = rho1;
@@ -336,8 +359,9 @@ constexpr size_t HCHUNK = 1024;  // steps per force readback
 struct lbm_gray {
     lbm_gray_setup setup{};
     gray::GParams p{};
-    bool fp64 = false;
-    size_t rsz = 4;
+    int storage = LBM_STORAGE_FP32;
+    size_t ssz = 4;  // bytes per stored population
+    size_t rsz = 4;  // bytes per real (arithmetic, moments, adjoint)
     cudaStream_t stream = nullptr;
     cudaEvent_t ev = nullptr;
     std::vector<void *> allocs;
@@ -363,7 +387,8 @@ struct lbm_gray {
     uint32_t nblk() const { return (p.N + gray::BLK - 1) / gray::BLK; }
     uint64_t nbox() const { return (uint64_t)p.box_n[0] * p.box_n[1] * p.box_n[2]; }
     uint32_t box_blocks() const { return (uint32_t)((nbox() + gray::BLK - 1) / gray::BLK); }
-    size_t set_bytes() const { return (size_t)19 * p.NP * rsz; }
+    size_t set_bytes() const { return (size_t)19 * p.NP * ssz; }   // a population set (or checkpoint)
+    size_t lset_bytes() const { return (size_t)19 * p.NP * rsz; }  // an adjoint set
     void *dalloc(size_t bytes) {
         void *q = nullptr;
         ck(cudaMalloc(&q, std::max<size_t>(bytes, 16)), "cudaMalloc");
@@ -396,15 +421,18 @@ struct lbm_gray {
             if (el > 1e-3) std::this_thread::sleep_for(std::chrono::microseconds(50));
         }
     }
+    // fn((S *)nullptr) with S the population storage type
     template <class F>
     void typed(F &&fn) {
-        if (fp64) fn((double *)nullptr); else fn((float *)nullptr);
+        if (storage == LBM_STORAGE_FP64) fn((double *)nullptr);
+        else if (storage == LBM_STORAGE_FP16) fn((__half *)nullptr);
+        else fn((float *)nullptr);
     }
     void reset() {
         typed([&](auto *t) {
-            using R = std::remove_pointer_t<decltype(t)>;
-            gray::kg_init<R><<<nblk(), gray::BLK, 0, stream>>>(p, (R *)P[0]);
-            gray::kg_init<R><<<nblk(), gray::BLK, 0, stream>>>(p, (R *)P[1]);
+            using S = std::remove_pointer_t<decltype(t)>;
+            gray::kg_init<S><<<nblk(), gray::BLK, 0, stream>>>(p, (S *)P[0]);
+            gray::kg_init<S><<<nblk(), gray::BLK, 0, stream>>>(p, (S *)P[1]);
         });
         ck(cudaGetLastError(), "init kernel");
         cur = 0;
@@ -412,17 +440,23 @@ struct lbm_gray {
     }
     // one forward step: faces on the current set, bulk into the other; out:
     // null (no forces) or 8 doubles for the force and moment of the step
+    // stochastic-rounding seed of step steps_done + 1 (the engine's rule)
+    uint32_t seed_mix() const {
+        const uint32_t seed = (uint32_t)((steps_done + 1) * 2654435761ull);
+        return seed * 0x85EBCA77u + 0x632BE5ABu;
+    }
     void step(void *mom_slot, double *out) {
         typed([&](auto *t) {
-            using R = std::remove_pointer_t<decltype(t)>;
-            const uint32_t rows = p.NY * p.NZ;
-            gray::kg_faces<R><<<(rows + gray::BLK - 1) / gray::BLK, gray::BLK, 0, stream>>>(p, (R *)P[cur]);
-            const R *src = (const R *)P[cur];
-            R *dst = (R *)P[1 - cur];
-            if (mom_slot && out) gray::kg_step<R, true, true><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, (R *)mom_slot, (R *)fbox);
-            else if (mom_slot) gray::kg_step<R, true, false><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, (R *)mom_slot, nullptr);
-            else if (out) gray::kg_step<R, false, true><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, nullptr, (R *)fbox);
-            else gray::kg_step<R, false, false><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, nullptr, nullptr);
+            using S = std::remove_pointer_t<decltype(t)>;
+            using R = typename gray::GS<S>::R;
+            const uint32_t rows = p.NY * p.NZ, mix = seed_mix();
+            gray::kg_faces<S><<<(rows + gray::BLK - 1) / gray::BLK, gray::BLK, 0, stream>>>(p, (S *)P[cur]);
+            const S *src = (const S *)P[cur];
+            S *dst = (S *)P[1 - cur];
+            if (mom_slot && out) gray::kg_step<S, true, true><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, (R *)mom_slot, (R *)fbox, mix);
+            else if (mom_slot) gray::kg_step<S, true, false><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, (R *)mom_slot, nullptr, mix);
+            else if (out) gray::kg_step<S, false, true><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, nullptr, (R *)fbox, mix);
+            else gray::kg_step<S, false, false><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, nullptr, nullptr, mix);
             if (out) gray::kg_force<R><<<box_blocks(), gray::BLK, 0, stream>>>(p, (const R *)fbox, partials, ticket, out);
         });
         ck(cudaGetLastError(), "step kernel");
@@ -485,7 +519,7 @@ double lbm_gray::backward(const lbm_adjoint_spec &sp, double *grad_out) {
     }
     const uint64_t kbase = all_kept ? 0 : K;  // first moment slot of the kept steps
     auto kept_slot = [&](uint64_t step1) { return (char *)mom + (kbase + (step1 - keep_from - 1)) * mom_bytes; };
-    if (!L[0]) { L[0] = dalloc(set_bytes()); L[1] = dalloc(set_bytes()); }
+    if (!L[0]) { L[0] = dalloc(lset_bytes()); L[1] = dalloc(lset_bytes()); }
     const uint64_t nb = nbox();
     if (!grad) grad = (double *)dalloc(std::max<uint64_t>(nb, 1) * 8);
     cudaEvent_t e0, e1;
@@ -524,8 +558,8 @@ double lbm_gray::backward(const lbm_adjoint_spec &sp, double *grad_out) {
     for (uint64_t s2 = sp.t0; s2 <= sp.t1; s2++) J += dsum[s2];
     J /= (double)(sp.t1 - sp.t0 + 1);
     // reverse sweep
-    ck(cudaMemsetAsync(L[0], 0, set_bytes(), stream), "adjoint init");
-    ck(cudaMemsetAsync(L[1], 0, set_bytes(), stream), "adjoint init");
+    ck(cudaMemsetAsync(L[0], 0, lset_bytes(), stream), "adjoint init");
+    ck(cudaMemsetAsync(L[1], 0, lset_bytes(), stream), "adjoint init");
     ck(cudaMemsetAsync(grad, 0, std::max<uint64_t>(nb, 1) * 8, stream), "gradient init");
     const double swin = 1.0 / (double)(sp.t1 - sp.t0 + 1);
     uint32_t lc = 0;  // L[lc] = lambda of step s+1
@@ -535,6 +569,7 @@ double lbm_gray::backward(const lbm_adjoint_spec &sp, double *grad_out) {
         if (!kept) {
             ck(cudaEventRecord(e0, stream), "cudaEventRecord");
             ck(cudaMemcpyAsync(P[cur], (char *)ckpt + seg * set_bytes(), set_bytes(), cudaMemcpyDeviceToDevice, stream), "restore");
+            steps_done = c;  // the recomputed steps round with the first pass's seeds
             for (uint64_t s2 = c; s2 < cend; s2++) step((char *)mom + (s2 - c) * mom_bytes, nullptr);
             t_rec += elapsed();
         }
@@ -543,7 +578,7 @@ double lbm_gray::backward(const lbm_adjoint_spec &sp, double *grad_out) {
             const void *mslot = kept ? (const void *)kept_slot(s2) : (const void *)((char *)mom + (s2 - 1 - c) * mom_bytes);
             const double sw = (s2 >= sp.t0 && s2 <= sp.t1) ? swin : 0.0;
             typed([&](auto *tp) {
-                using R = std::remove_pointer_t<decltype(tp)>;
+                using R = typename gray::GS<std::remove_pointer_t<decltype(tp)>>::R;
                 gray::kg_adjoint<R><<<nblk(), gray::BLK, 0, stream>>>(p, (const R *)L[lc], (R *)L[1 - lc], (const R *)mslot, grad, sp.objective, (R)sw);
             });
             ck(cudaGetLastError(), "adjoint kernel");
@@ -595,15 +630,17 @@ void create_gray(const lbm_gray_setup *s, lbm_gray *h) {
     const uint64_t N = (uint64_t)s->dims[0] * s->dims[1] * s->dims[2];
     if (s->dims[0] < 4 || s->dims[1] < 1 || s->dims[2] < 1) throw GErr(LBM_ERR_INVALID, "grid must be at least 4 cells along x");
     if (N >= 0x7fffffffull) throw GErr(LBM_ERR_INVALID, "grid of " + std::to_string(N) + " cells is out of range");
-    if (s->storage != LBM_STORAGE_FP32 && s->storage != LBM_STORAGE_FP64) throw GErr(LBM_ERR_UNSUPPORTED, "the gray lattice stores FP32 or FP64");
+    if (s->storage != LBM_STORAGE_FP32 && s->storage != LBM_STORAGE_FP64 && s->storage != LBM_STORAGE_FP16)
+        throw GErr(LBM_ERR_UNSUPPORTED, "the gray lattice stores FP32, FP64 or FP16");
     if (!(s->nu > 0.0)) throw GErr(LBM_ERR_INVALID, "viscosity must be positive");
     if (!(s->alpha > 0.0 && s->alpha <= 1.0)) throw GErr(LBM_ERR_INVALID, "alpha must be in (0, 1]");
     for (int k = 0; k < 3; k++)
         if (s->box_n[k] == 0 || (uint64_t)s->box_lo[k] + s->box_n[k] > s->dims[k]) throw GErr(LBM_ERR_INVALID, "design box outside the grid");
     if (s->box_lo[0] < 1 || s->box_lo[0] + s->box_n[0] > s->dims[0] - 1) throw GErr(LBM_ERR_INVALID, "design box must leave the x faces out");
     h->setup = *s;
-    h->fp64 = s->storage == LBM_STORAGE_FP64;
-    h->rsz = h->fp64 ? 8 : 4;
+    h->storage = s->storage;
+    h->rsz = s->storage == LBM_STORAGE_FP64 ? 8 : 4;
+    h->ssz = s->storage == LBM_STORAGE_FP64 ? 8 : (s->storage == LBM_STORAGE_FP16 ? 2 : 4);
     gray::GParams &p = h->p;
     p.NX = s->dims[0]; p.NY = s->dims[1]; p.NZ = s->dims[2]; p.N = (uint32_t)N;
     p.NP = (N + 255) / 256 * 256;
@@ -664,7 +701,7 @@ int lbm_gray_set_field(lbm_gray *h, const double *gamma) {
             const uint32_t x = (uint32_t)(b % p.box_n[0]), y = (uint32_t)((b / p.box_n[0]) % p.box_n[1]), z = (uint32_t)(b / ((uint64_t)p.box_n[0] * p.box_n[1]));
             a[((uint64_t)(p.box_lo[2] + z) * p.NY + p.box_lo[1] + y) * p.NX + p.box_lo[0] + x] = h->setup.alpha * g;
         }
-        if (h->fp64) {
+        if (h->rsz == 8) {
             ck(cudaMemcpyAsync(h->a, a.data(), a.size() * 8, cudaMemcpyHostToDevice, h->stream), "field upload");
             h->wait();
         } else {

@@ -61,6 +61,9 @@ class GraySetup:
     def nbox(self) -> int:
         return int(np.prod([int(v) for v in self.box_n]))
 
+    def cells(self) -> int:
+        return int(np.prod([int(v) for v in self.dims]))
+
     def to_c(self) -> _GraySetup:
         s = _GraySetup()
         s.dims[:] = [int(v) for v in self.dims]

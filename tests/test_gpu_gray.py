@@ -7,7 +7,10 @@ design cells through the torch.autograd.Function harness.  Tolerances: FP64
 engine vs oracle 1e-10 relative; recompute vs keep-all bit-equal; FP32 vs
 FP64 gradient 2e-3 relative L2 (small case), 1e-2 (full case); adjoint vs
 finite differences 1e-4 relative to the largest component (FP64) and 2e-2
-(FP32)."""
+(FP32).  FP16-stored forward (FP32 arithmetic and adjoint) against FP32:
+forces 2e-3 relative to the largest, gradient 2e-2 relative L2; its
+recompute sweep against its keep-all sweep bit-equal (the stochastic
+rounding repeats from the step's seed)."""
 import numpy as np
 import pytest
 
@@ -98,3 +101,29 @@ def test_design_case_gradient_against_central_differences():
     scale = np.max(np.abs(fd))
     assert np.max(np.abs(fd - g64[cells])) <= 1e-4 * scale
     assert np.max(np.abs(fd - g32[cells])) <= 2e-2 * scale
+
+
+def test_fp16_storage_forward_close_to_fp32():
+    s16, g = small(Storage.FP16)
+    s32, _ = small(Storage.FP32)
+    f16, f32 = GrayLattice(s16, g).run(60), GrayLattice(s32, g).run(60)
+    assert np.isfinite(f16).all()
+    assert np.max(np.abs(f16 - f32)) <= 2e-3 * np.max(np.abs(f32))
+
+
+def test_fp16_storage_recompute_equals_keep_all():
+    s, g = small(Storage.FP16)
+    e = GrayLattice(s, g)
+    J1, g1 = e.backward(AdjointSpec(steps=37, t0=5, t1=37, checkpoint_every=8, objective=1, dir=[0.3, 1.0, 0.2], recompute=True))
+    J2, g2 = e.backward(AdjointSpec(steps=37, t0=5, t1=37, checkpoint_every=8, objective=1, dir=[0.3, 1.0, 0.2], recompute=False))
+    assert J1 == J2 and np.array_equal(g1, g2)
+
+
+def test_fp16_storage_adjoint_close_to_fp32():
+    s16, g = small(Storage.FP16)
+    s32, _ = small(Storage.FP32)
+    spec = AdjointSpec(steps=60, t0=30, t1=60, checkpoint_every=20)
+    J16, g16 = GrayLattice(s16, g).backward(spec)
+    J32, g32 = GrayLattice(s32, g).backward(spec)
+    assert abs(J16 / J32 - 1.0) <= 2e-3
+    assert rel_l2(g16, g32) <= 2e-2
