@@ -851,10 +851,10 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 template <class S, int P, int COLL>
-__global__ void __launch_bounds__(BLOCK) k_walls(const __grid_constant__ LatParams p, const __grid_constant__ StepParams s) {
+__global__ void __launch_bounds__(WBLOCK) k_walls(const __grid_constant__ LatParams p, const __grid_constant__ StepParams s) {
     using R = typename Pop<S>::real;
     const Consts<R> &k = K<R>(p);
-    const uint32_t r = blockIdx.x * BLOCK + threadIdx.x;
+    const uint32_t r = blockIdx.x * WBLOCK + threadIdx.x;
     R Fo[3] = {0, 0, 0}, To[3] = {0, 0, 0};
     if (r < p.nrec) {
         const uint32_t cell = p.recs[r * RS + R_CELL];
@@ -918,7 +918,7 @@ __global__ void __launch_bounds__(BLOCK) k_walls(const __grid_constant__ LatPara
         }
     }
     // FP64 sum: warp shuffle -> block -> last block over all block partials
-    __shared__ double sh[BLOCK / 32][6];
+    __shared__ double sh[WBLOCK / 32][6];
     __shared__ bool last;
     double v[6] = {(double)Fo[0], (double)Fo[1], (double)Fo[2], (double)To[0], (double)To[1], (double)To[2]};
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -929,7 +929,7 @@ __global__ void __launch_bounds__(BLOCK) k_walls(const __grid_constant__ LatPara
     __syncthreads();
     if (threadIdx.x < 6) {
         double t = 0;
-        for (int w = 0; w < BLOCK / 32; w++) t += sh[w][threadIdx.x];
+        for (int w = 0; w < WBLOCK / 32; w++) t += sh[w][threadIdx.x];
         p.partials[blockIdx.x * 8 + threadIdx.x] = t;
         __threadfence();
     }
@@ -942,7 +942,7 @@ __global__ void __launch_bounds__(BLOCK) k_walls(const __grid_constant__ LatPara
     if (!last) return;
     __threadfence();
     double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (uint32_t b = threadIdx.x; b < gridDim.x; b += BLOCK)
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += WBLOCK)
         for (int j = 0; j < 6; j++) acc[j] += __ldcg(&p.partials[b * 8 + j]);
 #pragma unroll
     for (int j = 0; j < 6; j++) acc[j] = warp_sum(acc[j]);
@@ -952,7 +952,7 @@ __global__ void __launch_bounds__(BLOCK) k_walls(const __grid_constant__ LatPara
     __syncthreads();
     if (threadIdx.x < 6) {
         double t = 0;
-        for (int w = 0; w < BLOCK / 32; w++) t += sh[w][threadIdx.x];
+        for (int w = 0; w < WBLOCK / 32; w++) t += sh[w][threadIdx.x];
         p.hist[s.slot * 8 + threadIdx.x] = t;
     }
     if (threadIdx.x == 0) *p.ticket = 0u;
@@ -1172,13 +1172,13 @@ static cudaError_t step_t(const LatParams &p, const StepParams &s, cudaStream_t 
     if (overlap) {
         cudaEventRecord(fork, st);
         cudaStreamWaitEvent(side, fork, 0);
-        k_walls<S, P, COLL><<<blocks_for(p.nrec), BLOCK, 0, side>>>(p, s);
+        k_walls<S, P, COLL><<<(unsigned)((p.nrec + WBLOCK - 1) / WBLOCK), WBLOCK, 0, side>>>(p, s);
         cudaEventRecord(join, side);
     }
     if (s.nface) k_faces<S, P><<<blocks_for(s.nface), BLOCK, 0, st>>>(p, s);
     if (ev) cudaEventRecord(ev[1], st);
     if (overlap) cudaStreamWaitEvent(st, join, 0);
-    else if (p.nrec) k_walls<S, P, COLL><<<blocks_for(p.nrec), BLOCK, 0, st>>>(p, s);
+    else if (p.nrec) k_walls<S, P, COLL><<<(unsigned)((p.nrec + WBLOCK - 1) / WBLOCK), WBLOCK, 0, st>>>(p, s);
     if (ev) cudaEventRecord(ev[2], st);
     if (p.tma) {
         if (!p.forcing && !p.abs_u) {

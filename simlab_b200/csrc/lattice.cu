@@ -460,7 +460,7 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     p.recd = st.storage == LBM_STORAGE_FP64 ? (double *)h->dalloc(nrec * lbm::RD * 8) : nullptr;
     p.faces = (uint32_t *)h->dalloc(faces.size() * 4);
     p.face_info = (uint32_t *)h->dalloc(finfo.size() * 4);
-    const uint64_t nwb = (nrec + lbm::BLOCK - 1) / lbm::BLOCK;
+    const uint64_t nwb = (nrec + lbm::WBLOCK - 1) / lbm::WBLOCK;  // blocks of the wall-cell kernel
     p.partials = (double *)h->dalloc(std::max<uint64_t>(nwb, 1) * 8 * sizeof(double));
     p.ticket = (uint32_t *)h->dalloc(16);
     p.hist = (double *)h->dalloc(KMAX * 8 * sizeof(double));

@@ -49,6 +49,10 @@ constexpr uint32_t RS = 40, R_MASK = 0, R_CELL = 1, R_Q = 2, R_FPOST = 11, R_MAC
 constexpr uint32_t RD = 28, RD_FPOST = 0, RD_MACRO = 18, RD_FT = 22;
 
 constexpr int BLOCK = 256;
+#ifndef LBM_WBLOCK
+#define LBM_WBLOCK 256
+#endif
+constexpr int WBLOCK = LBM_WBLOCK;  // threads per block of the wall-cell kernel
 // flag bit of a fluid cell whose x neighbour is a planar x-face cell it feeds
 constexpr uint32_t FLAG_XFACE = 0x80000000u;
 constexpr uint32_t PLANE_ALIGN = 256;  // cells

@@ -91,6 +91,26 @@ def test_feature_case_fp32_parity(collision, wall_model):
     assert np.max(np.abs(rg[:, 11:33] - ro[:, 11:33])) < 1e-5
 
 
+@pytest.mark.parametrize("storage,tol", [(Storage.FP32, 1e-5), (Storage.FP16, 2e-3)])
+def test_lattice_smaller_than_one_tile(storage, tol):
+    """A 16x12x8 lattice (1,536 cells) is less than one tile of the staged
+    kernel (2,560 cells for 2-byte storage, 1,280 for 4-byte): one block, a
+    ragged tile clamped at both ends of every plane, x faces fused."""
+    dims = (16, 12, 8)
+    c = (7.3, 6.2, 3.9)
+    v, t = sphere(list(c), 2.6, 3)
+    vox = voxelize_static(v, t, list(dims))
+    F = FaceBc
+    st = LatticeSetup(dims=list(dims), faces=[F.VELOCITY, F.OPEN, F.FREE_SLIP, F.FREE_SLIP, F.FREE_SLIP, F.FREE_SLIP], nu=0.01,
+                      smagorinsky=0.17, u_inf=[0.04, 0.0, 0.0], u_init=[0.03, 0.002, 0.0], storage=storage, center=list(c), debug_dump=True)
+    g, o = _pair(st, vox)
+    hg, ho = g.run(80), o.run(80)
+    mg, mo = g.macros(), o.macros()
+    assert np.array_equal(np.isnan(mg[:, 0]), np.isnan(mo[:, 0]))
+    assert rel_l2(_u(mg), _u(mo)) <= tol
+    assert np.max(np.abs(hg - ho)) <= 10 * tol * np.max(np.abs(ho)) + 1e-9
+
+
 def test_fp64_engine_matches_fp64_oracle():
     st, vox = feature_case(Storage.FP64)
     g, o = _pair(st, vox, real64=True)
