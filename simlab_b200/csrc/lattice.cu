@@ -21,6 +21,10 @@
 #include "lbm_kernels.h"
 #include "voxel.hpp"
 
+#ifndef LBM_SIDE_PRIORITY
+#define LBM_SIDE_PRIORITY 1  // wall-cell stream at the device's greatest priority
+#endif
+
 namespace {
 
 thread_local std::string g_error;
@@ -561,7 +565,11 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     ck(cudaMemcpyAsync((void *)p.sp_tab, tabf.data(), tabf.size() * 4, cudaMemcpyHostToDevice, s), "upload sponge");
     ck(cudaMemcpyAsync((void *)p.sp_tabd, tabd.data(), tabd.size() * 8, cudaMemcpyHostToDevice, s), "upload sponge");
     if (walls_far) {
-        ck(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking), "cudaStreamCreate");
+        // the wall-cell kernel is the longer of the two that run before the
+        // bulk: its blocks go first on the SMs
+        int prio_lo = 0, prio_hi = 0;
+        ck(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi), "cudaDeviceGetStreamPriorityRange");
+        ck(cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, LBM_SIDE_PRIORITY ? prio_hi : prio_lo), "cudaStreamCreate");
         ck(cudaEventCreateWithFlags(&h->fork, cudaEventDisableTiming), "cudaEventCreate");
         ck(cudaEventCreateWithFlags(&h->join, cudaEventDisableTiming), "cudaEventCreate");
     }
