@@ -173,19 +173,24 @@ def time_storage(storage, steps, warmup, ws, with_profile):
 
 
 def e2e_time(lat, steps):
-    """Through the C-ABI call a caller makes (lbm_run with host buffers): per
-    step the StepIn goes host->device with the launch and the step's force
-    and moment come back to the host."""
+    """Through the C-ABI call a caller makes (lbm_run with host buffers), in
+    the batches the reference's study loop passes to Lattice::run
+    (tunnel.rs:1072: 0.25 x 2800e6 / cells steps, clamped to 16..4096): every
+    step's StepIn goes host->device with its launch and every step's force and
+    moment come back to the host before the call returns."""
     from simlab_b200.lbm import STEP_DTYPE, steps_array
 
-    one = steps_array(1)
+    batch = int(min(max(0.25 * 2800e6 / lat.setup.cells(), 16), 4096))
     lat.synchronize()
+    done = 0
     t0 = time.perf_counter()
-    for _ in range(steps):
-        f = lat.run(one)
+    while done < steps:
+        m = min(batch, steps - done)
+        f = lat.run(steps_array(m))
+        done += m
     t1 = time.perf_counter()
     assert np.all(np.isfinite(f))
-    return (t1 - t0) * 1e3, STEP_DTYPE.itemsize, 6 * 8
+    return (t1 - t0) * 1e3, STEP_DTYPE.itemsize, 6 * 8, batch
 
 
 def cpu_sample(storage, sample_s: float = 12.0, warm: int = 1):
@@ -445,10 +450,10 @@ def main():
         if kt:
             r["kernel_times"] = kt
         if headline:
-            e_ms, hb, db = e2e_time(lat, args.steps)
+            e_ms, hb, db, e_batch = e2e_time(lat, args.steps)
             e_ms = max_over_ranks(e_ms, ws)
             e2e = {"value": round(info["cells"] * args.steps * ws / (e_ms * 1e-3) / 1e6, 3), "unit": UNIT, "h2d_bytes_per_step": hb,
-                   "d2h_bytes_per_step": db}
+                   "d2h_bytes_per_step": db, "steps_per_call": e_batch}
         lat.close()
         del lat
         results[storage] = r
