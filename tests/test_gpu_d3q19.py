@@ -328,3 +328,21 @@ def test_arm_les_full_size_drag_vs_fp64():
         assert bad == 0 and np.all(np.isfinite(h)), s
         fx = window_mean(h)[0]
         assert abs(fx / fx64 - 1.0) < 5e-3, (s, fx, fx64)
+
+
+def test_at_scale_fp16_lattice_steps_finite():
+    """The at-scale case: 1024x512x512 FP16 (268 M cells, 11 GB) around the
+    arm scaled x2 runs without a non-finite value, keeps its mass to 1e-3
+    over 8 steps (inflow and outflow balance at the start) and gives finite
+    forces."""
+    from simlab_b200.cases import arm_les
+
+    st, vox = arm_les(Storage.FP16, scale=2)
+    g = Lattice(st, vox)
+    m0, b0 = g.mass()
+    f = g.run(8)
+    m1, b1 = g.mass()
+    g.close()
+    assert b0 == 0 and b1 == 0
+    assert np.isfinite(f).all()
+    assert abs(m1 / m0 - 1.0) < 1e-3
