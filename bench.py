@@ -115,8 +115,12 @@ def dist_init():
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+        backend = os.environ.get("SIMLAB_BENCH_BACKEND") or ("nccl" if torch.cuda.is_available() else "gloo")
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+        else:  # the host-side plumbing on CPU (tests): replicas, barrier, max over ranks
+            dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
     return ws, rank, local
 
 
@@ -133,7 +137,7 @@ def max_over_ranks(v: float, ws: int) -> float:
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    t = torch.tensor([v], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
