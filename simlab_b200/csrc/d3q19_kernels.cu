@@ -23,6 +23,7 @@
 
 #include "lbm_device.cuh"
 #include "lbm_kernels.h"
+#include "tma.cuh"
 #include "revoxel.cuh"
 
 namespace lbm {
@@ -472,45 +473,6 @@ __host__ __device__ __forceinline__ constexpr int lead(int j) {
     return (P == 0 || j == 0) ? 0 : (CX(j) == 1 ? 1 : (CX(j) == -1 ? (int)(16 / sizeof(S)) - 1 : 0));
 }
 
-__device__ __forceinline__ uint32_t smem_addr(const void *ptr) { return (uint32_t)__cvta_generic_to_shared(ptr); }
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
-    asm volatile("mbarrier.arrive.release.cta.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
-}
-// One test of the phase; a thread whose phase is not complete is suspended
-// until it completes or about a millisecond passes (the suspend-time hint),
-// instead of spinning on the test.
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity), "r"(1000000u)
-        : "memory");
-    return ok != 0;
-}
-__device__ __forceinline__ uint64_t global_ns() {
-    uint64_t t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-// bounded wait: false after limit_ns (about two seconds by default; at most
-// 2^22 tests)
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, uint64_t limit_ns = 2000000000ull) {
-    if (mbar_try_wait(bar, parity)) return true;
-    const uint64_t t0 = global_ns();
-    for (uint32_t it = 0; it < (1u << 22); it++) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if ((it & 63u) == 63u && global_ns() - t0 > limit_ns) return false;  // the clock every 64 tests
-    }
-    return false;
-}
-
 // Self-test of the bounded wait: one thread waits for a barrier phase that
 // nothing completes (no arrival, no copy); the wait must give up after
 // limit_ns and report it, and the context stays usable.  status[0] = 1 when
@@ -527,18 +489,6 @@ __global__ void k_wait_selftest(uint32_t *status, uint64_t limit_ns) {
         status[1] = us > 0xffffffffull ? 0xffffffffu : (uint32_t)us;
     }
 }
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
-                 : "memory");
-}
-__device__ __forceinline__ void bulk_s2g(void *dst, const void *src, uint32_t bytes) {
-    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(smem_addr(src)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // signed element shift of plane j's slots relative to the cell at parity P
 template <int P>

@@ -321,34 +321,17 @@ template <bool WRAP> struct StepOcc<double, WRAP> { static constexpr int value =
 // WRAP: the level has periodic axes (neighbour offsets per thread); without
 // them no stepped cell touches the boundary, and every neighbour offset is
 // uniform across the grid
-template <class S, bool FORCE, bool WRAP>
-__global__ void __launch_bounds__(BLK, StepOcc<S, WRAP>::value) k27_step(const __grid_constant__ LevelParams p, const StepArgs a) {
+// One cell's update once its 27 pulled populations f (storage units) are
+// in registers: walls, cumulant collision, stores into the other set, the
+// moments the neighbouring levels read (mshader.rs:199-403,612-699).
+template <class S, bool FORCE>
+__device__ __forceinline__ void cell27(const LevelParams &p, const StepArgs &a, uint32_t n, uint32_t fg, uint32_t x, uint32_t y, uint32_t z,
+                                       typename Pop<S>::real *f) {
     using R = typename Pop<S>::real;
-    const uint32_t n = blockIdx.x * BLK + threadIdx.x;
-    if (n >= p.N) return;
-    const uint32_t fg = p.flags[n];
-    if ((fg & 7u) != 0) return;
     const Consts27<R> &k = K<R>(p);
     const R SC = (R)Raw<S>::SC, ISC = (R)1 / (R)Raw<S>::SC;
-    uint32_t x, y, z;
-    coords(p, n, x, y, z);
-    const S *src = set_ptr<S>(p, a.src);
-    const S *srcn = src + n;
-    const int64_t NP = (int64_t)p.NP, SX = 1, SY = (int64_t)p.NX, SZ = (int64_t)p.NX * p.NY;
-    R f[27];
-    if (WRAP) {
-        // offsets of the axis neighbours with periodic wrap (mshader.rs:135-138)
-        const int32_t nx = (int32_t)p.NX, nxy = (int32_t)(p.NX * p.NY);
-        const int32_t xo[3] = {x == 0 ? nx - 1 : -1, 0, x == p.NX - 1 ? -(nx - 1) : 1};
-        const int32_t yo[3] = {y == 0 ? (int32_t)(p.NY - 1) * nx : -nx, 0, y == p.NY - 1 ? -(int32_t)(p.NY - 1) * nx : nx};
-        const int32_t zo[3] = {z == 0 ? (int32_t)(p.NZ - 1) * nxy : -nxy, 0, z == p.NZ - 1 ? -(int32_t)(p.NZ - 1) * nxy : nxy};
-#pragma unroll
-        for (int i = 0; i < 27; i++) f[i] = Raw<S>::ld(srcn + ((int64_t)i * NP + (xo[1 - CX(i)] + yo[1 - CY(i)] + zo[1 - CZ(i)])));
-    } else {
-        // pull: the population moving along c_i comes from n - c_i
-#pragma unroll
-        for (int i = 0; i < 27; i++) f[i] = Raw<S>::ld(srcn + ((int64_t)i * NP - CX(i) * SX - CY(i) * SY - CZ(i) * SZ));
-    }
+    const S *srcn = set_ptr<S>(p, a.src) + n;
+    const int64_t NP = (int64_t)p.NP;
     const uint32_t rec = fg >> 3;
     if (rec != 0) {
         // Bouzidi bounce-back with moving-wall momentum exchange (mshader.rs:364-403)
@@ -506,6 +489,36 @@ __global__ void __launch_bounds__(BLK, StepOcc<S, WRAP>::value) k27_step(const _
         for (int c = 0; c < 6; c++) o[4 + c] = pst[c];
         o[10] = tau;
     }
+}
+
+
+template <class S, bool FORCE, bool WRAP>
+__global__ void __launch_bounds__(BLK, StepOcc<S, WRAP>::value) k27_step(const __grid_constant__ LevelParams p, const StepArgs a) {
+    using R = typename Pop<S>::real;
+    const uint32_t n = blockIdx.x * BLK + threadIdx.x;
+    if (n >= p.N) return;
+    const uint32_t fg = p.flags[n];
+    if ((fg & 7u) != 0) return;
+    uint32_t x, y, z;
+    coords(p, n, x, y, z);
+    const S *src = set_ptr<S>(p, a.src);
+    const S *srcn = src + n;
+    const int64_t NP = (int64_t)p.NP, SX = 1, SY = (int64_t)p.NX, SZ = (int64_t)p.NX * p.NY;
+    R f[27];
+    if (WRAP) {
+        // offsets of the axis neighbours with periodic wrap (mshader.rs:135-138)
+        const int32_t nx = (int32_t)p.NX, nxy = (int32_t)(p.NX * p.NY);
+        const int32_t xo[3] = {x == 0 ? nx - 1 : -1, 0, x == p.NX - 1 ? -(nx - 1) : 1};
+        const int32_t yo[3] = {y == 0 ? (int32_t)(p.NY - 1) * nx : -nx, 0, y == p.NY - 1 ? -(int32_t)(p.NY - 1) * nx : nx};
+        const int32_t zo[3] = {z == 0 ? (int32_t)(p.NZ - 1) * nxy : -nxy, 0, z == p.NZ - 1 ? -(int32_t)(p.NZ - 1) * nxy : nxy};
+#pragma unroll
+        for (int i = 0; i < 27; i++) f[i] = Raw<S>::ld(srcn + ((int64_t)i * NP + (xo[1 - CX(i)] + yo[1 - CY(i)] + zo[1 - CZ(i)])));
+    } else {
+        // pull: the population moving along c_i comes from n - c_i
+#pragma unroll
+        for (int i = 0; i < 27; i++) f[i] = Raw<S>::ld(srcn + ((int64_t)i * NP - CX(i) * SX - CY(i) * SY - CZ(i) * SZ));
+    }
+    cell27<S, FORCE>(p, a, n, fg, x, y, z, f);
 }
 
 // ------------------------------------------------------------ level kernels
