@@ -487,7 +487,7 @@ def main():
                    "storage": "fp16 (f - w) x 32768, stochastic rounding", "parallelism": "replicas" if ws > 1 else "single GPU",
                    "l2": "inputs larger than L2 (1.41 GB of populations per replica)"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
-                     "traffic": traffic, "kernel": "k_bulk<fp16>", "bytes_per_lup": BYTES_PER_LUP[Storage.FP16],
+                     "traffic": traffic, "kernel": "k_bulk_tma<fp16>", "bytes_per_lup": BYTES_PER_LUP[Storage.FP16],
                      "kernel_ms": round(bulk_ms, 5), "peak_source": peak_kind},
         "storages": {s.name.lower(): {"mlups": round(r["mlups"], 3), "ms_per_step": round(r["ms_per_step"], 5),
                                       "hbm_frac_step": round(BYTES_PER_LUP[s] * cells * r["mlups"] / cells / 1e3 / hbm, 4)}
@@ -496,7 +496,8 @@ def main():
         "clocks": clocks,
         "e2e": e2e,
         "gpu_launches": 3 * args.steps,
-        "kernel_share": {k: round(v / max(kt["faces_ms"] + kt["walls_ms"] + kt["bulk_ms"], 1e-12), 4) for k, v in kt.items() if k != "steps"},
+        "kernel_share": {k.removesuffix("_ms"): round(v / max(kt["faces_ms"] + kt["walls_ms"] + kt["bulk_ms"], 1e-12), 4)
+                         for k, v in kt.items() if k != "steps"},
     }
     if ws == 1 and not args.no_extras:
         line["adjoint"] = adjoint_ratio()

@@ -369,7 +369,11 @@ __global__ void __launch_bounds__(BLOCK) k_faces(const __grid_constant__ LatPara
     const uint32_t m = (cz * p.NY + cy) * p.NX + cx;
     const bool fluid = (p.flags[m] & 3u) == 0u;
     R g[19], f[19];
-    if (fluid) load_prev_out<S, Q>(p, m, make_nb(p, cx, cy, cz), g);
+    // Loaded whatever the neighbour's flag says, so that these loads and the
+    // flag's go out together: the addresses depend only on m (make_nb wraps at
+    // the lattice's edges), and face_values ignores g when the neighbour is
+    // not fluid.
+    load_prev_out<S, Q>(p, m, make_nb(p, cx, cy, cz), g);
     face_values<R>(p, K<R>(p), info, fluid, g, f);
     Rng rng{sr_hash_mix(b, s.seed_mix)};
     store_prev_out<S, Q>(p, b, make_nb(p, x, y, z), info >> 8, f, rng);
