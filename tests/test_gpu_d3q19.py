@@ -188,6 +188,21 @@ def test_checkpoint_round_trip_is_exact():
     assert np.array_equal(a, b)
 
 
+def test_zero_steps_change_nothing():
+    """Lattice::run with an empty step list returns no forces; neither it nor
+    advance(0) touches the state or the step count."""
+    st, vox = feature_case(Storage.FP16)
+    g = Lattice(st, vox)
+    g.run(5)
+    blob = g.save_state()
+    out = g.run(0)
+    g.advance(0)
+    g.synchronize()
+    assert out.shape == (0, 6)
+    assert g.steps_done == 5
+    assert g.save_state() == blob
+
+
 def test_macros_needs_debug_dump():
     st, vox = feature_case()
     st.debug_dump = False
