@@ -444,19 +444,24 @@ int lbm_gray_stream(lbm_gray *h, void **stream);
 
 /* Allocation-free force and moment sum over wall records (no counterpart in
  * the reference).  For callers that cannot allocate device memory where they
- * need the sum: code running during CUDA graph capture, hosts whose device
- * memory comes from their own pool allocator, embedded callers with a fixed
- * footprint.  records_dev: nrec records of 40 u32 words in device memory
- * (the layout of lbm_records); forces_dev: 6 doubles in device memory
- * (force, then moment); stream: a cudaStream_t (NULL for the default
- * stream).  The call enqueues the work and returns; it allocates and frees
- * nothing.  Scratch: a fixed array inside this library, 256 KiB on every
- * device that loads it, kept until the process exits and shared by all calls
- * on that device: calls whose work overlaps on the GPU race and must be
- * ordered by the caller.  At most lbm_record_forces_noalloc_max() records
- * (1,048,576); more is rejected with LBM_ERR_INVALID.  The first call on a
- * device looks up the scratch address and should come before any stream
- * capture.  Errors: message from lbm_noalloc_error. */
+ * need the sum: hosts whose device memory is all handed out by their own pool
+ * allocator, embedded callers with a fixed device footprint, latency-critical
+ * loops that cannot afford cudaMalloc/cudaFree (which may synchronise the
+ * device).  records_dev: nrec D3Q19 records of 40 u32 words in device memory
+ * (the layout of lbm_records; the 24-word records of lbm_multi_records are
+ * not accepted); forces_dev: 6 doubles in device memory (force, then moment);
+ * stream: a cudaStream_t (NULL for the default stream).  The sum is over the
+ * records' float force words in FP64, also for FP64-storage lattices (whose
+ * lbm_run forces sum the double copies, so the two differ at float rounding).
+ * The call enqueues the work and returns; it allocates and frees nothing.
+ * Scratch: a fixed array inside this library, 256 KiB on every device that
+ * loads it, kept until the process exits and shared by all calls on that
+ * device: calls whose work overlaps on the GPU race and must be ordered by
+ * the caller.  At most lbm_record_forces_noalloc_max() records (1,048,576);
+ * more is rejected with LBM_ERR_INVALID.  The first call on a device looks up
+ * the scratch's device address (kept for the life of the process, so the
+ * device's context must not be reset in between); make that first call
+ * before any stream capture.  Errors: message from lbm_noalloc_error. */
 int lbm_record_forces_noalloc(const uint32_t *records_dev, uint64_t nrec, double *forces_dev, void *stream);
 uint64_t lbm_record_forces_noalloc_max(void);
 int lbm_noalloc_error(char *buf, uint64_t len);

@@ -47,6 +47,8 @@ inline double weight19(int i) { return i == 0 ? 1.0 / 3.0 : (i <= 6 ? 1.0 / 18.0
 
 // record layout, shader.rs:62-69
 constexpr uint32_t RS = 40, R_MASK = 0, R_CELL = 1, R_Q = 2, R_FPOST = 11, R_MACRO = 29, R_FT = 33;
+constexpr float FP16_SCALE = 32768.0f;          // shader.rs:73
+constexpr uint32_t STEP_SEED_MUL = 2654435761u;  // lattice.rs:676
 
 // ---------------------------------------------------------------- bit helpers
 inline uint32_t fbits(float x) { uint32_t b; std::memcpy(&b, &x, 4); return b; }
@@ -187,7 +189,7 @@ struct D3Q19 {
         switch (storage) {
             case LBM_STORAGE_FP32: return (Real)p32[k];
             case LBM_STORAGE_FP64: return (Real)p64[k];
-            case LBM_STORAGE_FP16: return (Real)(f16_to_f32(p16[k]) * (1.0f / 32768.0f));
+            case LBM_STORAGE_FP16: return (Real)(f16_to_f32(p16[k]) * (1.0f / FP16_SCALE));
             default: return (Real)bf16_to_f32(p16[k]);
         }
     }
@@ -196,7 +198,7 @@ struct D3Q19 {
         switch (storage) {
             case LBM_STORAGE_FP32: p32[k] = (float)v; break;
             case LBM_STORAGE_FP64: p64[k] = (double)v; break;
-            case LBM_STORAGE_FP16: p16[k] = f32_to_f16(sround16((float)v * 32768.0f, key, seed)); break;
+            case LBM_STORAGE_FP16: p16[k] = f32_to_f16(sround16((float)v * FP16_SCALE, key, seed)); break;
             default: p16[k] = f32_to_bf16(sround_bf16((float)v, key, seed)); break;
         }
     }
@@ -889,7 +891,7 @@ struct D3Q19 {
     // force and moment summed over all records (FP64, record order)
     std::array<double, 6> step(const lbm_step_in &sin) {
         int p = (int)(steps_done % 2);
-        seed = (uint32_t)steps_done * 2654435761u;  // lattice.rs:676
+        seed = (uint32_t)steps_done * STEP_SEED_MUL;  // lattice.rs:676
         Real omega[3] = {(Real)sin.omega[0], (Real)sin.omega[1], (Real)sin.omega[2]};
         if (moving) {
             float rot[9], rotp[9];
@@ -912,7 +914,7 @@ struct D3Q19 {
     // the z-planes [z0, z1) (no faces, the step counter is not advanced)
     void step_slab(uint32_t z0, uint32_t z1) {
         int p = (int)(steps_done % 2);
-        seed = (uint32_t)steps_done * 2654435761u;
+        seed = (uint32_t)steps_done * STEP_SEED_MUL;
         Real omega[3] = {0, 0, 0};
         uint64_t a = (uint64_t)z0 * NX * NY, b = (uint64_t)std::min(z1, NZ) * NX * NY;
 #pragma omp parallel for schedule(static)

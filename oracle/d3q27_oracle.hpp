@@ -58,6 +58,7 @@ inline double weight(int i) {
 constexpr uint32_t RS = 24, R_MASK = 0, R_CELL = 1, R_Q = 2, R_FT = 15, MW = 12;
 constexpr uint32_t T_FLUID = 0, T_SOLID = 1, T_FACE = 2, T_GHOST = 3, T_RESTRICT = 4;
 constexpr size_t HIST_CAP = 1024;  // mlattice.rs:283
+constexpr uint32_t SEED_SRC_MUL = 7919u, SEED_MW_MUL = 104729u;  // mlattice.rs:704
 
 }  // namespace q27
 
@@ -124,7 +125,7 @@ struct Multi27 {
         switch (storage) {
             case LBM_STORAGE_FP32: return (Real)l.p32[set][k];
             case LBM_STORAGE_FP64: return (Real)l.p64[set][k];
-            case LBM_STORAGE_FP16: return (Real)(f16_to_f32(l.p16[set][k]) * (1.0f / 32768.0f));
+            case LBM_STORAGE_FP16: return (Real)(f16_to_f32(l.p16[set][k]) * (1.0f / FP16_SCALE));
             default: return (Real)bf16_to_f32(l.p16[set][k]);
         }
     }
@@ -134,7 +135,7 @@ struct Multi27 {
         switch (storage) {
             case LBM_STORAGE_FP32: l.p32[set][k] = (float)v; break;
             case LBM_STORAGE_FP64: l.p64[set][k] = (double)v; break;
-            case LBM_STORAGE_FP16: l.p16[set][k] = f32_to_f16(sround16((float)v * 32768.0f, key, seed)); break;
+            case LBM_STORAGE_FP16: l.p16[set][k] = f32_to_f16(sround16((float)v * FP16_SCALE, key, seed)); break;
             default: l.p16[set][k] = f32_to_bf16(sround_bf16((float)v, key, seed)); break;
         }
     }
@@ -531,7 +532,7 @@ struct Multi27 {
 
     // mlattice.rs:692-703
     uint32_t seed_of(uint32_t hslot, uint32_t src, uint32_t mw) const {
-        return ((uint32_t)fine_steps + hslot) * 2654435761u + (src * 7919u + mw * 104729u);
+        return ((uint32_t)fine_steps + hslot) * STEP_SEED_MUL + (src * q27::SEED_SRC_MUL + mw * q27::SEED_MW_MUL);
     }
 
     // ------------------------------------------------------------ kernels

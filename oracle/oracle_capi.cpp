@@ -152,6 +152,39 @@ unsigned long long orc_steps_done(void *hp) {
 
 // the FP16 / BF16 conversions and the stochastic rounding, exposed so the
 // tests can check them against known values
+// The constant tables the oracle computes with, for the test that pins them
+// against the reference's source text: D3Q19 velocities (3 ints each),
+// opposites, weights and record layout {RS, R_MASK, R_CELL, R_Q, R_FPOST,
+// R_MACRO, R_FT}; D3Q27 velocities, opposites, slots, weights and
+// {RS, R_MASK, R_CELL, R_Q, R_FT, MW, T_FLUID, T_SOLID, T_FACE, T_GHOST,
+// T_RESTRICT}; scalars {FP16_SCALE, STEP_SEED_MUL, SEED_SRC_MUL, SEED_MW_MUL}.
+int orc_tables(int *c19, int *opp19, double *w19, uint32_t *rec19, int *c27, int *opp27, int *slot27, double *w27, uint32_t *rec27,
+               double *scalars) {
+    for (int i = 0; i < 19; i++) {
+        for (int k = 0; k < 3; k++) c19[3 * i + k] = oracle::C19[i][k];
+        opp19[i] = oracle::opp19(i);
+        w19[i] = oracle::weight19(i);
+    }
+    const uint32_t r19[7] = {oracle::RS, oracle::R_MASK, oracle::R_CELL, oracle::R_Q, oracle::R_FPOST, oracle::R_MACRO, oracle::R_FT};
+    for (int k = 0; k < 7; k++) rec19[k] = r19[k];
+    namespace q = oracle::q27;
+    for (int i = 0; i < 27; i++) {
+        c27[3 * i] = q::cx(i);
+        c27[3 * i + 1] = q::cy(i);
+        c27[3 * i + 2] = q::cz(i);
+        opp27[i] = q::opp(i);
+        slot27[i] = q::slot(i);
+        w27[i] = q::weight(i);
+    }
+    const uint32_t r27[11] = {q::RS, q::R_MASK, q::R_CELL, q::R_Q, q::R_FT, q::MW, q::T_FLUID, q::T_SOLID, q::T_FACE, q::T_GHOST, q::T_RESTRICT};
+    for (int k = 0; k < 11; k++) rec27[k] = r27[k];
+    scalars[0] = oracle::FP16_SCALE;
+    scalars[1] = oracle::STEP_SEED_MUL;
+    scalars[2] = q::SEED_SRC_MUL;
+    scalars[3] = q::SEED_MW_MUL;
+    return 0;
+}
+uint32_t orc_sr_hash(uint32_t key, uint32_t seed) { return oracle::sr_hash(key, seed); }
 uint16_t orc_f32_to_f16(float x) { return oracle::f32_to_f16(x); }
 float orc_f16_to_f32(uint16_t h) { return oracle::f16_to_f32(h); }
 uint16_t orc_f16_bits_ref(float x) { return oracle::f16_bits_ref(x); }

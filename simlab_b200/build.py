@@ -55,16 +55,25 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     objdir = PKG / "_build"
     objdir.mkdir(exist_ok=True)
     log: list[str] = []
-    objs = []
     cc = nvcc()
+    cmds = []
     for src in CUDA_SOURCES:
         obj = objdir / (src + ".o")
-        _run([cc, *ARCH, *NVCC_FLAGS, "-I", str(ROOT / "include"), "-c", str(CSRC / src), "-o", str(obj)], log)
-        objs.append(str(obj))
+        cmds.append(([cc, *ARCH, *NVCC_FLAGS, "-I", str(ROOT / "include"), "-c", str(CSRC / src), "-o", str(obj)], obj))
     for src in CXX_SOURCES:
         obj = objdir / (src + ".o")
-        _run(["g++", "-O3", "-std=c++17", "-fPIC", "-fopenmp", "-c", str(CSRC / src), "-o", str(obj)], log)
-        objs.append(str(obj))
+        cmds.append((["g++", "-O3", "-std=c++17", "-fPIC", "-fopenmp", "-c", str(CSRC / src), "-o", str(obj)], obj))
+    # the translation units are independent: compile them side by side
+    from concurrent.futures import ThreadPoolExecutor
+
+    logs: list[list[str]] = [[] for _ in cmds]
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        futs = [ex.submit(_run, c, logs[k]) for k, (c, _) in enumerate(cmds)]
+        for f in futs:
+            f.result()
+    for lg in logs:
+        log.extend(lg)
+    objs = [str(o) for _, o in cmds]
     tmp = LIB.with_suffix(".so.tmp")
     _run([cc, *ARCH, "-shared", "-o", str(tmp), *objs, "-Xcompiler", "-fopenmp", "-lgomp", "-lcudart"], log)
     os.replace(tmp, LIB)

@@ -748,7 +748,7 @@ __global__ void __launch_bounds__(Tma<S>::threads, Tma<S>::min_blocks) k_bulk_tm
                 continue;
             }
             // FP16 values stay in storage units (x 32768) through the collision
-            constexpr int SC = std::is_same<S, __half>::value ? 32768 : 1;
+            constexpr int SC = std::is_same<S, __half>::value ? (int)FP16_SCALE : 1;
             R f[19];
 #pragma unroll
             for (int i = 0; i < 19; i++) {

@@ -18,8 +18,26 @@
 
 namespace lbm27 {
 
+// velocity set (d3q27.rs:1-29): direction i has velocity (i%3-1, (i/3)%3-1,
+// i/9-1), the rest population is 13, the opposite of i is 26-i, and SLOT
+// numbers the moving directions 0..25 in per-link arrays
+__host__ __device__ __forceinline__ constexpr int CX(int i) { return i % 3 - 1; }
+__host__ __device__ __forceinline__ constexpr int CY(int i) { return (i / 3) % 3 - 1; }
+__host__ __device__ __forceinline__ constexpr int CZ(int i) { return i / 9 - 1; }
+__host__ __device__ __forceinline__ constexpr int OPP27(int i) { return 26 - i; }
+__host__ __device__ __forceinline__ constexpr int SLOT(int i) { return i < 13 ? i : i - 1; }
+__host__ __device__ __forceinline__ constexpr double WD(int i) {
+    return (CX(i) * CX(i) + CY(i) * CY(i) + CZ(i) * CZ(i)) == 0 ? 8.0 / 27.0
+         : (CX(i) * CX(i) + CY(i) * CY(i) + CZ(i) * CZ(i)) == 1 ? 2.0 / 27.0
+         : (CX(i) * CX(i) + CY(i) * CY(i) + CZ(i) * CZ(i)) == 2 ? 1.0 / 54.0
+                                                                 : 1.0 / 216.0;
+}
+
 constexpr uint32_t RS = 24, R_MASK = 0, R_CELL = 1, R_Q = 2, R_FT = 15;  // record words (mshader.rs:32-36)
 constexpr uint32_t MW = 12;                                               // words per exported moment node
+// terms of a level step's rounding seed (mlattice.rs:704): (finest step + slot)
+// * 2654435761 + source set * 7919 + moment slot * 104729
+constexpr uint32_t SEED_SRC_MUL = 7919u, SEED_MW_MUL = 104729u;
 constexpr uint32_t T_FLUID = 0, T_SOLID = 1, T_FACE = 2, T_GHOST = 3, T_RESTRICT = 4;
 
 template <class R>

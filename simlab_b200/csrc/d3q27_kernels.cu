@@ -36,16 +36,6 @@ using lbm::Rng;
 
 constexpr int BLK = 256;
 
-__host__ __device__ __forceinline__ constexpr int CX(int i) { return i % 3 - 1; }
-__host__ __device__ __forceinline__ constexpr int CY(int i) { return (i / 3) % 3 - 1; }
-__host__ __device__ __forceinline__ constexpr int CZ(int i) { return i / 9 - 1; }
-__host__ __device__ __forceinline__ constexpr int SLOT(int i) { return i < 13 ? i : i - 1; }
-__host__ __device__ __forceinline__ constexpr double WD(int i) {
-    return (CX(i) * CX(i) + CY(i) * CY(i) + CZ(i) * CZ(i)) == 0 ? 8.0 / 27.0
-         : (CX(i) * CX(i) + CY(i) * CY(i) + CZ(i) * CZ(i)) == 1 ? 2.0 / 27.0
-         : (CX(i) * CX(i) + CY(i) * CY(i) + CZ(i) * CZ(i)) == 2 ? 1.0 / 54.0
-                                                                 : 1.0 / 216.0;
-}
 template <class R> __device__ __forceinline__ R W(int i) { return (R)WD(i); }
 template <> __device__ __forceinline__ float W<float>(int i) { return (float)WD(i); }
 template <class R> __device__ __forceinline__ R W45(int i) { return (R)(4.5 * WD(i)); }
@@ -217,7 +207,7 @@ template <> struct Raw<double> {
     static __device__ __forceinline__ void st1(double *a, double va, Rng &) { *a = va; }
 };
 template <> struct Raw<__half> {
-    static constexpr float SC = 32768.0f;
+    static constexpr float SC = lbm::FP16_SCALE;
     static __device__ __forceinline__ float ld(const __half *p) { return __half2float(*p); }
     // one stochastically rounding conversion per pair
     static __device__ __forceinline__ void st2(__half *a, float va, __half *b, float vb, Rng &r) {

@@ -193,9 +193,9 @@ void fill_consts(lbm::Consts<R> &k, const lbm_setup &st) {
 
 lbm::StepParams step_params(const lbm_lattice *h, const lbm_step_in &s, uint32_t slot, uint64_t step_index) {
     lbm::StepParams sp{};
-    sp.seed = (uint32_t)step_index * 2654435761u;  // lattice.rs:676
+    sp.seed = (uint32_t)step_index * lbm::STEP_SEED_MUL;  // lattice.rs:676
     sp.seed_mix = sp.seed * 0x85EBCA77u + 0x632BE5ABu;
-    sp.next_seed_mix = ((uint32_t)(step_index + 1) * 2654435761u) * 0x85EBCA77u + 0x632BE5ABu;
+    sp.next_seed_mix = ((uint32_t)(step_index + 1) * lbm::STEP_SEED_MUL) * 0x85EBCA77u + 0x632BE5ABu;
     sp.nface = h->fused_valid ? h->nface_rest : h->nface;
     sp.slot = slot;
     for (int a = 0; a < 3; a++) {

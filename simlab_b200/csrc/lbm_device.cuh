@@ -43,6 +43,11 @@ __host__ __device__ __forceinline__ constexpr int DIR(int x, int y, int z) {
     return r;
 }
 
+// FP16 storage scale (shader.rs:73) and the step seed multiplier of the
+// stochastic rounding (lattice.rs:676: seed = step * 2654435761)
+constexpr float FP16_SCALE = 32768.0f;
+constexpr uint32_t STEP_SEED_MUL = 2654435761u;
+
 // record layout (u32 words per wall record), shader.rs:62-69
 constexpr uint32_t RS = 40, R_MASK = 0, R_CELL = 1, R_Q = 2, R_FPOST = 11, R_MACRO = 29, R_FT = 33;
 // FP64 engine keeps the float fields of a record in doubles: 18 fpost, 4 macro, 6 ft
@@ -224,7 +229,7 @@ __device__ __forceinline__ uint32_t pair_bits(uint32_t h) {
 // FP16 stores (f - w) * 32768 (binary16's range holds the deviations with
 // the scale; values beyond it saturate)
 __device__ __forceinline__ __half sr_f16(float v, Rng &r) {
-    return __ushort_as_half((unsigned short)(cvt_rs_f16x2(v * 32768.0f, 0.0f, r.next()) >> 16));
+    return __ushort_as_half((unsigned short)(cvt_rs_f16x2(v * FP16_SCALE, 0.0f, r.next()) >> 16));
 }
 // BF16 stores (f - w) as is
 __device__ __forceinline__ __nv_bfloat16 sr_bf16(float v, Rng &r) {
@@ -249,7 +254,7 @@ template <> struct Pop<double> {
 // in storage units (values already scaled), bits(x) reinterprets 16 bits
 template <> struct Pop<__half> {
     using real = float;
-    static __device__ __forceinline__ float cvt(__half v) { return __half2float(v) * (1.0f / 32768.0f); }
+    static __device__ __forceinline__ float cvt(__half v) { return __half2float(v) * (1.0f / FP16_SCALE); }
     static __device__ __forceinline__ float ld(const __half *p) { return cvt(*p); }
     static __device__ __forceinline__ __half enc(float v, Rng &r) { return sr_f16(v, r); }
     static __device__ __forceinline__ uint32_t rs2(float a, float b, uint32_t bits) { return cvt_rs_f16x2(a, b, bits); }

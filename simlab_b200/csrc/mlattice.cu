@@ -120,7 +120,7 @@ struct lbm_multi {
     }
     size_t sub_steps() const { return (size_t)1 << (lv.size() - 1); }
     uint32_t seed_of(uint32_t hslot, uint32_t src, uint32_t mw) const {  // mlattice.rs:692-703
-        return ((uint32_t)fine_steps + hslot) * 2654435761u + (src * 7919u + mw * 104729u);
+        return ((uint32_t)fine_steps + hslot) * lbm::STEP_SEED_MUL + (src * lbm27::SEED_SRC_MUL + mw * lbm27::SEED_MW_MUL);
     }
     static uint32_t mix(uint32_t seed) { return seed * 0x85EBCA77u + 0x632BE5ABu; }
 

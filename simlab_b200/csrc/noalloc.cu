@@ -1,16 +1,20 @@
 // Force and moment sum over wall records without any device allocation.
 //
 // Some callers cannot allocate device memory at the point where they need
-// this sum: code running while a stream is being captured into a CUDA graph
-// (cudaMalloc is not allowed there), hosts whose device memory is handed out
-// by their own pool allocator, or embedded callers that must keep a fixed
-// footprint.  lbm_record_forces_noalloc sums the force and moment words of
-// wall records that already live in device memory (the layout lbm_records
-// returns) into six doubles in device memory, using only a scratch area that
-// is part of this library's image: a file-scope __device__ array of a fixed,
-// modest size that every GPU loading the library keeps until the process
-// exits.  The caller passes the inputs and the output; nothing is allocated
-// or freed.
+// this sum: hosts whose device memory is all handed out by their own pool
+// allocator, embedded callers that must keep a fixed device footprint, and
+// latency-critical loops that cannot afford cudaMalloc/cudaFree, which may
+// synchronise the whole device.  lbm_record_forces_noalloc sums the force and
+// moment words of wall records that already live in device memory (the
+// 40-word D3Q19 layout lbm_records returns) into six doubles in device
+// memory, using only a scratch area that is part of this library's image: a
+// file-scope __device__ array of a fixed, modest size that every GPU loading
+// the library keeps until the process exits.  The caller passes the inputs
+// and the output; nothing is allocated or freed.
+//
+// The sum is over the records' float force words (FP32 values summed in
+// FP64), also for FP64-storage lattices, whose lbm_run forces sum the double
+// copies instead; the two then differ at float rounding.
 //
 // The scratch is shared by every call on a device and keeps the last call's
 // contents; each call clears the counter it needs before using it.  Two calls
@@ -23,13 +27,16 @@
 #include <string>
 
 #include "../../include/simlab_lbm.h"
+#include "lbm_device.cuh"
 
 namespace {
 
 constexpr uint32_t NA_BLOCK = 256;
 constexpr uint64_t NA_MAX_RECORDS = 1ull << 20;                   // 1,048,576 records
 constexpr uint32_t NA_MAX_BLOCKS = (uint32_t)(NA_MAX_RECORDS / NA_BLOCK);  // 4096
-constexpr uint32_t REC_WORDS = 40, REC_FT = 33;                   // record layout (F at 33..35, T at 36..38)
+// the engine's D3Q19 record layout (force at R_FT..R_FT+2, moment after it)
+constexpr uint32_t REC_WORDS = lbm::RS, REC_FT = lbm::R_FT;
+static_assert(REC_WORDS == 40 && REC_FT + 6 <= REC_WORDS, "wall record layout of lbm_records");
 
 struct NoallocScratch {
     double partials[NA_MAX_BLOCKS * 8];  // per-block sums (6 used of 8), 256 KiB
@@ -86,7 +93,10 @@ __global__ void __launch_bounds__(NA_BLOCK) k_record_sum(const uint32_t *recs, u
 }
 
 std::mutex g_mu;
-NoallocScratch *g_ptr[64] = {};  // scratch address per device, found once per device
+// scratch address per device ordinal, found once per device; this assumes
+// the device's primary context lives as long as the process (a
+// cudaDeviceReset would leave a stale address here)
+NoallocScratch *g_ptr[64] = {};
 thread_local std::string g_err;
 
 }  // namespace

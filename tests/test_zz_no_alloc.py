@@ -1,9 +1,10 @@
 """The allocation-free record sum (lbm_record_forces_noalloc) against the
 force and moment lbm_run returns for the same step.
 
-Callers that cannot allocate device memory at the point of use (during CUDA
-graph capture, under their own pool allocator, with a fixed footprint) call
-this entry point with device pointers only.  The test puts a lattice's wall
+Callers that cannot allocate device memory at the point of use (a host whose
+device memory belongs to its own pool allocator, an embedded caller with a
+fixed footprint, a loop that cannot afford cudaMalloc/cudaFree) call this
+entry point with device pointers only.  The test puts a lattice's wall
 records into device memory, calls the entry point twice in a row through the
 C ABI and compares each result with lbm_run's force and moment of the step
 the records come from (FP64 sums of the same float words, so to 1e-12).
