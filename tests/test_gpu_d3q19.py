@@ -328,21 +328,29 @@ def test_gpu_periodic_sphere_array_stokes_drag():
 # ------------------------------------------------------------------ full size
 def test_arm_les_full_size_drag_vs_fp64():
     """The 512x256x256 LES arm: FP32, FP16 and BF16 storage against the FP64
-    engine over 3000 steps, mean drag over the last 65 % of the run (the
-    averaging window of crates/cfd/src/tunnel.rs:1065) within 0.5 %, and every
-    density finite."""
+    engine over 3000 steps, mean drag and lift over the last 65 % of the run
+    (the averaging window of crates/cfd/src/tunnel.rs:1065), every density
+    finite.  Drag within 0.5 %; lift, which this beam makes small (3.5 % of
+    the drag), within 0.5 % of the drag (its coefficient error measured on the
+    drag coefficient's scale, as q and A are the same).  The FP64 engine from
+    a perturbed initial state (1e-6 of the inflow speed) gives the flow's own
+    noise floor over this window, which must stay far below the bar."""
     from simlab_b200.cases import arm_les
     from simlab_b200.validate import run_case, window_mean
 
     steps = 3000
     ref, _, bad = run_case(lambda s: arm_les(s), Storage.FP64, steps)
     assert bad == 0 and np.all(np.isfinite(ref))
-    fx64 = window_mean(ref)[0]
+    m64 = window_mean(ref)
+    fl, _, bad = run_case(lambda s: arm_les(s), Storage.FP64, steps, perturbed=1.0)
+    mfl = window_mean(fl)
+    assert abs(mfl[0] / m64[0] - 1.0) < 1e-5 and abs(mfl[2] - m64[2]) / abs(m64[0]) < 1e-5, (mfl, m64)
     for s in (Storage.FP32, Storage.FP16, Storage.BF16):
         h, _, bad = run_case(lambda s: arm_les(s), s, steps)
         assert bad == 0 and np.all(np.isfinite(h)), s
-        fx = window_mean(h)[0]
-        assert abs(fx / fx64 - 1.0) < 5e-3, (s, fx, fx64)
+        m = window_mean(h)
+        assert abs(m[0] / m64[0] - 1.0) < 5e-3, (s, m[0], m64[0])
+        assert abs(m[2] - m64[2]) / abs(m64[0]) < 5e-3, (s, m[2], m64[2])
 
 
 def test_at_scale_fp16_lattice_steps_finite():
