@@ -41,6 +41,11 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "MLUPS (D3Q19 LES arm 512x256x256, FP16-stored populations)"
 UNIT = "MLUPS"
+DTYPE = "f32 arithmetic, fp16 storage"
+CONFIG = {"workload": "D3Q19 regularized + Smagorinsky LES (Cs 0.17), arm 200x12x8 + cylinder r10 h14, 512x256x256, "
+                      "u 0.05, Re 1e5, Bouzidi walls, wind-tunnel faces + sponges",
+          "storage": "fp16 (f - w) x 32768, stochastic rounding",
+          "l2": "inputs larger than L2 (1.41 GB of populations per replica)"}
 
 
 def peaks():
@@ -197,30 +202,52 @@ def e2e_time(lat, steps):
     return (t1 - t0) * 1e3, STEP_DTYPE.itemsize, 6 * 8, batch
 
 
-def cpu_sample(storage, sample_s: float = 12.0, warm: int = 1):
+ARM_FIXTURE = ROOT / "oracle" / "fixtures" / "arm_les_512x256x256.npz"
+CPU_SLAB = 8  # z-planes per CPU sample step
+
+
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+
+    return platform.processor() or "unknown"
+
+
+def cpu_oracle_sample(steps=None, warmup: int = 1, budget_s: float = 12.0):
     """The oracle (the reference's update restated in C++, OpenMP over all host
-    cores) on bounded samples of the same case: collide-stream over slabs of 8
-    z-planes of the full 512x256x256 lattice."""
+    cores) on the 512x256x256 arm case, loaded from its frozen inputs
+    (oracle/fixtures, written by oracle/make_arm_fixture.py) so that nothing of
+    the engine is imported or loaded.  One sample step is the collide-stream
+    over a slab of CPU_SLAB z-planes of the full lattice, cycling through z;
+    `steps` of them, or as many as fit in budget_s.  Both CPU figures (the
+    bench line's cpu_baseline and the --impl reference arm) come from here,
+    so they time the same work."""
     import oracle
-    from simlab_b200.cases import arm_les
 
     cores = oracle.set_threads(os.cpu_count() or 1)
-    st, vox = arm_les(storage)
-    lat = oracle.OracleLattice(st, vox)
-    nx, ny, nz = st.dims
-    slab = 8
-    for k in range(warm):
-        lat.step_slab(k * slab, (k + 1) * slab)
-    cells = 0
+    lat = oracle.OracleLattice.from_fixture(ARM_FIXTURE)
+    nx, ny, nz = (int(d) for d in lat.setup.dims)
+    slab = CPU_SLAB
     z = 0
-    t0 = time.perf_counter()
-    while time.perf_counter() - t0 < sample_s:
+    for _ in range(warmup):
         lat.step_slab(z, z + slab)
-        cells += nx * ny * slab
         z = (z + slab) % nz
+    n = 0
+    t0 = time.perf_counter()
+    while (n < steps) if steps is not None else (time.perf_counter() - t0 < budget_s):
+        lat.step_slab(z, z + slab)
+        z = (z + slab) % nz
+        n += 1
     dt = time.perf_counter() - t0
     lat.close()
-    return cells / dt / 1e6, cores, f"{cells // (nx * ny * slab)} slabs of {nx}x{ny}x{slab} cells in {dt:.1f} s"
+    v = nx * ny * slab * n / dt / 1e6
+    return {"value": round(v, 3), "unit": UNIT, "cores": cores, "kind": "port", "cpu": cpu_model(), "nproc": os.cpu_count(),
+            "sample": f"{n} slabs of {nx}x{ny}x{slab} cells of the 512x256x256 arm lattice (FP16 storage) in {dt:.1f} s"}, n, dt
 
 
 def adjoint_ratio():
@@ -386,33 +413,17 @@ def c5_adjoint():
 
 
 def run_reference(args, ws, rank):
+    """The reference arm: the oracle on the host cores, rank 0 only, on the
+    same workload, metric and config as the engine's line; each step one
+    sample step of cpu_oracle_sample."""
     if rank != 0:
         return
-    import oracle
-    from simlab_b200.cases import arm_les
-    from simlab_b200.lbm import Storage
-
-    cores = oracle.set_threads(os.cpu_count() or 1)
-    st, vox = arm_les(Storage.FP16)
-    lat = oracle.OracleLattice(st, vox)
-    nx, ny, nz = st.dims
-    slab = 2
-    for k in range(args.warmup):
-        lat.step_slab((k * slab) % nz, (k * slab) % nz + slab)
-    t0 = time.perf_counter()
-    for k in range(args.steps):
-        z = (k * slab) % nz
-        lat.step_slab(z, z + slab)
-    dt = time.perf_counter() - t0
-    v = nx * ny * slab * args.steps / dt / 1e6
-    sample = f"each step: collide-stream over {nx}x{ny}x{slab} cells of the 512x256x256 arm lattice (FP16 storage)"
-    line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+    cb, n, dt = cpu_oracle_sample(steps=args.steps, warmup=args.warmup)
+    v = cb["value"]
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / max(args.steps, 1), 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "D3Q19 LES arm 512x256x256 (oracle: the reference update restated in C++)", "storage": "fp16",
-                       "parallelism": "host threads"},
-            "cpu_baseline": {"value": round(v, 3), "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
-            "e2e": {"value": round(v, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "scaling": "weak", "vs_baseline": None, "dtype": DTYPE, "data": "synthetic", "config": CONFIG,
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -480,12 +491,10 @@ def main():
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32 arithmetic, fp16 storage",
+        "dtype": DTYPE,
         "data": "synthetic",
-        "config": {"workload": "D3Q19 regularized + Smagorinsky LES (Cs 0.17), arm 200x12x8 + cylinder r10 h14, 512x256x256, "
-                               "u 0.05, Re 1e5, Bouzidi walls, wind-tunnel faces + sponges",
-                   "storage": "fp16 (f - w) x 32768, stochastic rounding", "parallelism": "replicas" if ws > 1 else "single GPU",
-                   "l2": "inputs larger than L2 (1.41 GB of populations per replica)"},
+        "config": CONFIG,
+        "parallelism": "replicas" if ws > 1 else "single GPU",
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                      "traffic": traffic, "kernel": "k_bulk_tma<fp16>", "bytes_per_lup": BYTES_PER_LUP[Storage.FP16],
                      "kernel_ms": round(bulk_ms, 5), "peak_source": peak_kind},
@@ -495,9 +504,9 @@ def main():
         "fp16_over_fp32": round(h["mlups"] / results[Storage.FP32]["mlups"], 3),
         "clocks": clocks,
         "e2e": e2e,
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": int(kt["launches"]),
         "kernel_share": {k.removesuffix("_ms"): round(v / max(kt["faces_ms"] + kt["walls_ms"] + kt["bulk_ms"], 1e-12), 4)
-                         for k, v in kt.items() if k != "steps"},
+                         for k, v in kt.items() if k.endswith("_ms")},
     }
     if ws == 1 and not args.no_extras:
         line["adjoint"] = adjoint_ratio()
@@ -505,8 +514,7 @@ def main():
         line["c5_fp16_1024x512x512"] = c5_throughput()
         line["c5_adjoint"] = c5_adjoint()
     if rank == 0 and ws == 1 and not args.no_cpu:
-        v, cores, sample = cpu_sample(Storage.FP16)
-        line["cpu_baseline"] = {"value": round(v, 3), "unit": UNIT, "cores": cores, "kind": "port", "sample": sample}
+        line["cpu_baseline"] = cpu_oracle_sample(budget_s=12.0)[0]
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:

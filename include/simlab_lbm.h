@@ -209,13 +209,15 @@ int lbm_synchronize(lbm_lattice *h);
 
 /* Per-kernel device time of the steps enqueued while profiling is on,
  * from CUDA events recorded around each kernel on the handle's stream (no
- * reference counterpart; for the roofline figures).  Enabling clears the
- * totals; lbm_kernel_times waits for the stream and returns them. */
+ * reference counterpart; for the roofline figures), and the number of
+ * kernels those steps launched.  Enabling clears the totals;
+ * lbm_kernel_times waits for the stream and returns them. */
 typedef struct {
     uint64_t steps;
     double faces_ms;
     double walls_ms;
     double bulk_ms;
+    uint64_t launches;
 } lbm_kernel_times;
 int lbm_profile(lbm_lattice *h, int32_t enable);
 int lbm_get_kernel_times(lbm_lattice *h, lbm_kernel_times *out);

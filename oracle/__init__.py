@@ -65,14 +65,17 @@ class OracleLattice:
     real64=False: the reference's FP32 update; real64=True: the FP64 oracle
     (use Storage.FP64 in the setup for FP64 storage)."""
 
-    def __init__(self, setup, geometry=None, real64: bool = False):
-        from simlab_b200.lbm import geometry_struct  # the C-ABI structs are shared
-
+    def __init__(self, setup, geometry=None, real64: bool = False, _frozen=None):
         L = library()
         self._L = L
         self.setup = setup
         cs = setup.to_c()
-        g, keep = geometry_struct(geometry)
+        if _frozen is not None:  # a fixture's geometry (oracle.abi), no engine import
+            g, keep = _frozen
+        else:
+            from simlab_b200.lbm import geometry_struct  # the C-ABI structs are shared
+
+            g, keep = geometry_struct(geometry)
         h = L.orc_create(C.addressof(cs), C.addressof(g), int(real64))
         del keep
         if not h:
@@ -80,6 +83,16 @@ class OracleLattice:
             L.orc_last_error(buf, 1024)
             raise RuntimeError(buf.value.decode())
         self._h = h
+
+    @classmethod
+    def from_fixture(cls, path, real64: bool = False) -> "OracleLattice":
+        """The oracle on a frozen case (oracle/fixtures, written by
+        oracle/make_arm_fixture.py): setup and geometry come from the file,
+        nothing of the engine is imported or loaded."""
+        from .abi import load_case
+
+        setup, g, keep = load_case(Path(path))
+        return cls(setup, real64=real64, _frozen=(g, keep))
 
     def close(self):
         if getattr(self, "_h", None):

@@ -374,9 +374,48 @@ __global__ void __launch_bounds__(BLOCK) k_faces(const __grid_constant__ LatPara
     // the lattice's edges), and face_values ignores g when the neighbour is
     // not fluid.
     load_prev_out<S, Q>(p, m, make_nb(p, cx, cy, cz), g);
-    face_values<R>(p, K<R>(p), info, fluid, g, f);
     Rng rng{sr_hash_mix(b, s.seed_mix)};
-    store_prev_out<S, Q>(p, b, make_nb(p, x, y, z), info >> 8, f, rng);
+    const Nb nb = make_nb(p, x, y, z);
+    const uint32_t mask = info >> 8;
+    if ((info & 3u) == 2u) {  // free slip: the mirror image
+        face_values<R>(p, K<R>(p), info, fluid, g, f);
+        store_prev_out<S, Q>(p, b, nb, mask, f, rng);
+        return;
+    }
+    // velocity inlet or open face: face_values' state, then feq + fneq only in
+    // the directions stored (a planar face stores 5 of the 19)
+    const Consts<R> &k = K<R>(p);
+    R rho = 1, ux = k.u_inf[0], uy = k.u_inf[1], uz = k.u_inf[2];
+    R pi[6] = {0, 0, 0, 0, 0, 0};
+    if (fluid) {
+        const Moments<R> mo = moments<R>(g);
+        rho = (R)1 + mo.rho1;
+        ux = mo.jx / rho - (R)0.5 * k.grav[0];
+        uy = mo.jy / rho - (R)0.5 * k.grav[1];
+        uz = mo.jz / rho - (R)0.5 * k.grav[2];
+        pi_neq<R>(mo, rho, ux, uy, uz, pi);
+    }
+    if ((info & 3u) == 0u) {
+        if (p.total_p) {
+            const R uinf2 = k.u_inf[0] * k.u_inf[0] + k.u_inf[1] * k.u_inf[1] + k.u_inf[2] * k.u_inf[2];
+            rho = ((R)(1.0 / 3.0) + (R)0.5 * uinf2) / ((R)(1.0 / 3.0) + (R)0.5 * (ux * ux + uy * uy + uz * uz));
+        } else {
+            ux = k.u_inf[0]; uy = k.u_inf[1]; uz = k.u_inf[2];
+        }
+    } else {
+        rho = 1;
+    }
+    const R rho1 = rho - (R)1;
+    const R usq = (R)1.5 * (ux * ux + uy * uy + uz * uz);
+    const R tr = (pi[0] + pi[1] + pi[2]) * (R)(1.0 / 3.0);
+    S *pop = (S *)p.pop;
+#pragma unroll
+    for (int i = 0; i < 19; i++) {
+        if (!(mask & (1u << i))) continue;
+        const S v = Pop<S>::enc(feq_i<R>(i, rho1, rho, ux, uy, uz, usq) + fneq_i<R>(i, pi, tr), rng);
+        if (Q == 0 || i == 0) pop[(uint64_t)OPP(i) * p.NP + b] = v;
+        else pop[(uint64_t)i * p.NP + (uint32_t)((int32_t)b + nb.off(CX(i), CY(i), CZ(i)))] = v;
+    }
 }
 
 // ---------------------------------------------------------------- staged bulk
@@ -804,6 +843,89 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
+static_assert((RS * 4) % 16 == 0, "records are read with 16-byte loads");
+// The record's first 32 words (mask, cell, q, post-collision populations)
+// in eight 16-byte loads.
+__device__ __forceinline__ void record_words32(const LatParams &p, uint32_t r, uint32_t *w) {
+    const uint4 *rv = reinterpret_cast<const uint4 *>(p.recs + (uint64_t)r * RS);
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        const uint4 v = rv[q];
+        w[4 * q] = v.x; w[4 * q + 1] = v.y; w[4 * q + 2] = v.z; w[4 * q + 3] = v.w;
+    }
+}
+
+// The cut links of a wall-record cell (shader.rs:399-436): for every link i
+// of the mask, Bouzidi-Firdaouss-Lallemand interpolated bounce-back with the
+// moving-wall term overwrites f[opp i] (q >= 1/2 from the cell's last
+// post-collision values, q < 1/2 with the opposite link open also from its
+// input), and the Galilean-invariant momentum exchange (Wen et al. 2014) adds
+// the link's force and moment about the centre to Fo and To.  w: the record's
+// first 32 words; f: the cell's inputs; om receives the wall's angular
+// velocity.
+template <class R>
+__device__ __forceinline__ void wall_links(const LatParams &p, const StepParams &s, uint32_t r, const uint32_t *w, R pcx, R pcy, R pcz, R *f,
+                                           R *om, R *Fo, R *To) {
+    const uint32_t mask = w[R_MASK];
+    if (sizeof(R) == 8) { om[0] = (R)s.omega_d[0]; om[1] = (R)s.omega_d[1]; om[2] = (R)s.omega_d[2]; }
+    else { om[0] = (R)s.omega[0]; om[1] = (R)s.omega[1]; om[2] = (R)s.omega[2]; }
+    R fin[19];
+#pragma unroll
+    for (int i = 0; i < 19; i++) fin[i] = f[i];
+    // post-collision population i of the last step (FP64: the double copy) and q of link i
+    auto fpost = [&](int i) -> R {
+        if constexpr (sizeof(R) == 8) return Rec<R>::fpost(p, r, i);
+        else return __uint_as_float(w[R_FPOST + i - 1]);
+    };
+    auto qof = [&](int i) -> R {
+        const uint32_t qw = w[R_Q + (i - 1) / 2];
+        return (R)__half2float(__ushort_as_half((unsigned short)(((i - 1) & 1) ? (qw >> 16) : (qw & 0xffffu))));
+    };
+#pragma unroll
+    for (int i = 1; i < 19; i++) {
+        if (mask & (1u << i)) {
+            const int o = OPP(i);
+            const R wi = (R)WD(i);
+            const R q = max(qof(i), (R)0.001);
+            const R fpi = fpost(i) + wi;
+            const R fpo = fpost(o) + wi;
+            const R cx = (R)CX(i), cy = (R)CY(i), cz = (R)CZ(i);
+            const R xwx = pcx + q * cx, xwy = pcy + q * cy, xwz = pcz + q * cz;
+            const R uwx = om[1] * xwz - om[2] * xwy, uwy = om[2] * xwx - om[0] * xwz, uwz = om[0] * xwy - om[1] * xwx;
+            const R cu = cx * uwx + cy * uwy + cz * uwz;
+            R fb;
+            if (q >= (R)0.5) fb = (fpi + ((R)2 * q - (R)1) * fpo - (R)6 * wi * cu) / ((R)2 * q);
+            else if ((mask & (1u << o)) == 0u) fb = (R)2 * q * fpi + ((R)1 - (R)2 * q) * (fin[i] + wi) - (R)6 * wi * cu;
+            else fb = fpi - (R)6 * wi * cu;
+            f[o] = fb - wi;
+            const R flx = (cx - uwx) * fpi + (cx + uwx) * fb;
+            const R fly = (cy - uwy) * fpi + (cy + uwy) * fb;
+            const R flz = (cz - uwz) * fpi + (cz + uwz) * fb;
+            Fo[0] += flx; Fo[1] += fly; Fo[2] += flz;
+            To[0] += xwy * flz - xwz * fly;
+            To[1] += xwz * flx - xwx * flz;
+            To[2] += xwx * fly - xwy * flx;
+        }
+    }
+}
+
+// A wall-record cell's state after its collision written to its record
+// (shader.rs:437-441, 848-860): post-collision populations, rho and u, and the
+// step's force and moment (plus what a spinning part's re-voxelizer booked).
+template <class R>
+__device__ __forceinline__ void record_after(const LatParams &p, uint32_t r, const R *f, R rho, R ux, R uy, R uz, R *Fo, R *To) {
+#pragma unroll
+    for (int i = 1; i < 19; i++) Rec<R>::set_fpost(p, r, i, f[i]);
+    Rec<R>::set_macro(p, r, 0, rho);
+    Rec<R>::set_macro(p, r, 1, ux);
+    Rec<R>::set_macro(p, r, 2, uy);
+    Rec<R>::set_macro(p, r, 3, uz);
+    if (p.moving) {
+        for (int a = 0; a < 3; a++) { Fo[a] += Rec<R>::ft(p, r, a); To[a] += Rec<R>::ft(p, r, 3 + a); }
+    }
+    for (int a = 0; a < 3; a++) { Rec<R>::set_ft(p, r, a, Fo[a]); Rec<R>::set_ft(p, r, 3 + a, To[a]); }
+}
+
 template <class S, int P, int COLL>
 __global__ void __launch_bounds__(WBLOCK) k_walls(const __grid_constant__ LatParams p, const __grid_constant__ StepParams s) {
     using R = typename Pop<S>::real;
@@ -811,60 +933,29 @@ __global__ void __launch_bounds__(WBLOCK) k_walls(const __grid_constant__ LatPar
     const uint32_t r = blockIdx.x * WBLOCK + threadIdx.x;
     R Fo[3] = {0, 0, 0}, To[3] = {0, 0, 0};
     if (r < p.nrec) {
-        const uint32_t cell = p.recs[r * RS + R_CELL];
-        const uint32_t fg = cell < p.N ? p.flags[cell] : 1u;
-        if ((fg & 3u) == 0u && (fg >> 2) == r + 1u) {
-            uint32_t x, y, z;
-            coords(p, cell, x, y, z);
-            const Nb nb = make_nb(p, x, y, z);
-            R f[19];
-            load_in<S, P>(p, cell, nb, f);
-            R fin[19];
-#pragma unroll
-            for (int i = 0; i < 19; i++) fin[i] = f[i];
-            const uint32_t mask = p.recs[r * RS + R_MASK];
+        // The record's first 32 words, the cell's flag and its 19 populations
+        // issued together before anything waits on them: the wall kernel is
+        // short and latency-bound, so one round trip to HBM instead of a chain
+        // of dependent loads per cut link.
+        uint32_t w[32];
+        record_words32(p, r, w);
+        const uint32_t cell0 = w[R_CELL];
+        const bool inside = cell0 < p.N;
+        const uint32_t cell = inside ? cell0 : 0u;
+        const uint32_t fg = p.flags[cell];
+        uint32_t x, y, z;
+        coords(p, cell, x, y, z);
+        const Nb nb = make_nb(p, x, y, z);
+        R f[19];
+        load_in<S, P>(p, cell, nb, f);
+        if (inside && (fg & 3u) == 0u && (fg >> 2) == r + 1u) {
+            const uint32_t mask = w[R_MASK];
             const R pcx = (R)x - k.center[0], pcy = (R)y - k.center[1], pcz = (R)z - k.center[2];
             R om[3];
-            if (sizeof(R) == 8) { om[0] = (R)s.omega_d[0]; om[1] = (R)s.omega_d[1]; om[2] = (R)s.omega_d[2]; }
-            else { om[0] = (R)s.omega[0]; om[1] = (R)s.omega[1]; om[2] = (R)s.omega[2]; }
-#pragma unroll
-            for (int i = 1; i < 19; i++) {
-                if (mask & (1u << i)) {
-                    const int o = OPP(i);
-                    const R w = (R)WD(i);
-                    const R q = max((R)rec_q(p.recs, r, i), (R)0.001);
-                    const R fpi = Rec<R>::fpost(p, r, i) + w;
-                    const R fpo = Rec<R>::fpost(p, r, o) + w;
-                    const R cx = (R)CX(i), cy = (R)CY(i), cz = (R)CZ(i);
-                    const R xwx = pcx + q * cx, xwy = pcy + q * cy, xwz = pcz + q * cz;
-                    const R uwx = om[1] * xwz - om[2] * xwy, uwy = om[2] * xwx - om[0] * xwz, uwz = om[0] * xwy - om[1] * xwx;
-                    const R cu = cx * uwx + cy * uwy + cz * uwz;
-                    R fb;
-                    if (q >= (R)0.5) fb = (fpi + ((R)2 * q - (R)1) * fpo - (R)6 * w * cu) / ((R)2 * q);
-                    else if ((mask & (1u << o)) == 0u) fb = (R)2 * q * fpi + ((R)1 - (R)2 * q) * (fin[i] + w) - (R)6 * w * cu;
-                    else fb = fpi - (R)6 * w * cu;
-                    f[o] = fb - w;
-                    const R flx = (cx - uwx) * fpi + (cx + uwx) * fb;
-                    const R fly = (cy - uwy) * fpi + (cy + uwy) * fb;
-                    const R flz = (cz - uwz) * fpi + (cz + uwz) * fb;
-                    Fo[0] += flx; Fo[1] += fly; Fo[2] += flz;
-                    To[0] += xwy * flz - xwz * fly;
-                    To[1] += xwz * flx - xwx * flz;
-                    To[2] += xwx * fly - xwy * flx;
-                }
-            }
+            wall_links<R>(p, s, r, w, pcx, pcy, pcz, f, om, Fo, To);
             R rho, ux, uy, uz;
             relax<R, COLL>(p, k, f, x, y, z, true, r, mask, pcx, pcy, pcz, om, rho, ux, uy, uz);
-#pragma unroll
-            for (int i = 1; i < 19; i++) Rec<R>::set_fpost(p, r, i, f[i]);
-            Rec<R>::set_macro(p, r, 0, rho);
-            Rec<R>::set_macro(p, r, 1, ux);
-            Rec<R>::set_macro(p, r, 2, uy);
-            Rec<R>::set_macro(p, r, 3, uz);
-            if (p.moving) {
-                for (int a = 0; a < 3; a++) { Fo[a] += Rec<R>::ft(p, r, a); To[a] += Rec<R>::ft(p, r, 3 + a); }
-            }
-            for (int a = 0; a < 3; a++) { Rec<R>::set_ft(p, r, a, Fo[a]); Rec<R>::set_ft(p, r, 3 + a, To[a]); }
+            record_after<R>(p, r, f, rho, ux, uy, uz, Fo, To);
             Rng rng{sr_hash_mix(cell, s.seed_mix)};
             store_out<S, P>(p, cell, nb, f, rng);
         } else {

@@ -95,6 +95,7 @@ struct lbm_lattice {
     bool prof = false;
     std::vector<cudaEvent_t> prof_ev;
     uint64_t prof_steps = 0;
+    uint64_t prof_launches = 0;  // kernels launched by the profiled steps
     uint64_t pop_bytes = 0;
     uint32_t nface_rest = 0;   // face cells the face kernel handles once x faces are fused
     bool xfuse = false;        // planar x faces are written by the staged kernel
@@ -326,7 +327,7 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     // wall records (lattice.rs:454-482; record_words 202-218)
     const bool stat = geom && geom->kind == 1;
     const uint64_t nrec = stat ? geom->nwalls : 0;
-    if (nrec >= 0x3fffffffull) throw LbmError(LBM_ERR_INVALID, "too many wall records");
+    if (nrec > lbm::MAX_RECORDS) throw LbmError(LBM_ERR_INVALID, "too many wall records");
     h->nrec = (uint32_t)nrec;
     std::vector<uint32_t> words(nrec * lbm::RS, 0);
     std::vector<double> wordsd;
@@ -603,6 +604,9 @@ void run_impl(lbm_lattice *h, const lbm_step_in *steps, uint64_t n, double *forc
                 }
                 evs = h->prof_ev.data() + 4 * h->prof_steps;
                 h->prof_steps++;
+                // the kernels launch_step enqueues for this step
+                h->prof_launches += (sp.nface ? 1u : 0u) + (p.nrec ? 1u : 0u) + 1u + (p.moving ? 2u + (p.ntri ? 1u : 0u) : 0u);
+                if (si.sample) h->prof_launches += (h->nvert ? 1u : 0u) + (h->npix ? 1u : 0u);
             }
             ck(lbm::launch_step(h->setup.storage, p, sp, (int)(idx % 2), h->setup.collision, h->stream, h->side, h->fork, h->join, evs),
                "step kernels");
@@ -697,6 +701,7 @@ int lbm_profile(lbm_lattice *h, int32_t enable) {
         h->wait();
         h->prof = enable != 0;
         h->prof_steps = 0;
+        h->prof_launches = 0;
     });
 }
 
@@ -705,6 +710,7 @@ int lbm_get_kernel_times(lbm_lattice *h, lbm_kernel_times *out) {
     return guard(h, [&] {
         h->wait();
         out->steps = h->prof_steps;
+        out->launches = h->prof_launches;
         out->faces_ms = out->walls_ms = out->bulk_ms = 0.0;
         for (uint64_t k = 0; k < h->prof_steps; k++) {
             cudaEvent_t *e = h->prof_ev.data() + 4 * k;

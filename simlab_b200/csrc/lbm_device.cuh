@@ -55,11 +55,14 @@ constexpr uint32_t RD = 28, RD_FPOST = 0, RD_MACRO = 18, RD_FT = 22;
 
 constexpr int BLOCK = 256;
 #ifndef LBM_WBLOCK
-#define LBM_WBLOCK 256
+#define LBM_WBLOCK 64
 #endif
 constexpr int WBLOCK = LBM_WBLOCK;  // threads per block of the wall-cell kernel
 // flag bit of a fluid cell whose x neighbour is a planar x-face cell it feeds
 constexpr uint32_t FLAG_XFACE = 0x80000000u;
+// wall-record indices stay below 2^29, so the record field ((r + 1) << 2)
+// never reaches FLAG_XFACE
+constexpr uint32_t MAX_RECORDS = (1u << 29) - 2;
 constexpr uint32_t PLANE_ALIGN = 256;  // cells
 constexpr uint32_t TILE_MAX = 4096;    // cells of the staged kernel's largest tile (allocation guards)
 

@@ -137,7 +137,8 @@ STEP_DTYPE = np.dtype([("rot", "<f8", (3, 3)), ("rot_prev", "<f8", (3, 3)), ("om
 
 
 class _KernelTimes(C.Structure):
-    _fields_ = [("steps", C.c_uint64), ("faces_ms", C.c_double), ("walls_ms", C.c_double), ("bulk_ms", C.c_double)]
+    _fields_ = [("steps", C.c_uint64), ("faces_ms", C.c_double), ("walls_ms", C.c_double), ("bulk_ms", C.c_double),
+                ("launches", C.c_uint64)]
 
 
 class _Info(C.Structure):
@@ -518,7 +519,7 @@ class Lattice:
         """Device milliseconds per kernel summed over the profiled steps."""
         t = _KernelTimes()
         self._check(self._L.lbm_get_kernel_times(self._h, C.byref(t)))
-        return {"steps": int(t.steps), "faces_ms": t.faces_ms, "walls_ms": t.walls_ms, "bulk_ms": t.bulk_ms}
+        return {"steps": int(t.steps), "faces_ms": t.faces_ms, "walls_ms": t.walls_ms, "bulk_ms": t.bulk_ms, "launches": int(t.launches)}
 
     @property
     def stream(self) -> int:
