@@ -52,6 +52,9 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     deps = [CSRC / s for s in CUDA_SOURCES + CXX_SOURCES + HEADERS] + [ROOT / "include" / "simlab_lbm.h", Path(__file__)]
     if not force and not _stale(LIB, deps):
         return LIB
+    # the library is stamped with the newest source time seen now, so a source
+    # edited while the build runs leaves it stale for the next call
+    t_src = max(d.stat().st_mtime for d in deps)
     objdir = PKG / "_build"
     objdir.mkdir(exist_ok=True)
     log: list[str] = []
@@ -77,6 +80,7 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     tmp = LIB.with_suffix(".so.tmp")
     _run([cc, *ARCH, "-shared", "-o", str(tmp), *objs, "-Xcompiler", "-fopenmp", "-lgomp", "-lcudart"], log)
     os.replace(tmp, LIB)
+    os.utime(LIB, (t_src, t_src))
     (objdir / "build.log").write_text("\n".join(log))
     if verbose:
         print("\n".join(log))
