@@ -19,7 +19,7 @@ LIB = PKG / "libsimlab_lbm.so"
 
 CUDA_SOURCES = ["d3q19_kernels.cu", "lattice.cu", "noalloc.cu", "d3q27_kernels.cu", "mlattice.cu", "gray.cu"]
 CXX_SOURCES = ["voxel.cpp"]
-HEADERS = ["lbm_device.cuh", "lbm_kernels.h", "voxel.hpp", "d3q27.h", "revoxel.cuh", "spin_math.cuh", "tma.cuh"]
+HEADERS = ["lbm_device.cuh", "lbm_kernels.h", "voxel.hpp", "d3q27.h", "revoxel.cuh", "spin_math.cuh", "tma.cuh", "reduce.cuh"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-prec-div=false", "-prec-sqrt=false", "-Xcompiler", "-fPIC,-fopenmp",

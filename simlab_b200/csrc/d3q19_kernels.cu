@@ -24,6 +24,7 @@
 #include "lbm_device.cuh"
 #include "lbm_kernels.h"
 #include "tma.cuh"
+#include "reduce.cuh"
 #include "revoxel.cuh"
 
 namespace lbm {
@@ -1137,33 +1138,32 @@ __global__ void __launch_bounds__(BLOCK) k_sample_slices(const __grid_constant__
 // FP64 sum of rho over fluid cells (wall cells included) from the
 // post-collision populations of the last step, and a count of non-finite
 // densities.
+// Grid-stride over the cells (a few blocks per SM), each thread summing its
+// cells in order, then the deterministic grid sum of reduce.cuh: the same
+// result on every run, one atomic per block.  out[0] = mass, out[1] = the
+// count of non-finite densities.
 template <class S, int Q>
-__global__ void __launch_bounds__(BLOCK) k_mass(const __grid_constant__ LatParams p, double *mass, unsigned long long *bad) {
+__global__ void __launch_bounds__(BLOCK) k_mass(const __grid_constant__ LatParams p, double *scratch, double *out) {
     using R = typename Pop<S>::real;
-    const uint32_t n = blockIdx.x * BLOCK + threadIdx.x;
-    double v = 0;
-    unsigned nb_bad = 0;
-    if (n < p.N) {
+    double v = 0, nbad = 0;
+    const uint32_t stride = gridDim.x * BLOCK;
+#pragma unroll 1
+    for (uint32_t n = blockIdx.x * BLOCK + threadIdx.x; n < p.N; n += stride) {
         const uint32_t fg = p.flags[n];
-        if ((fg & 3u) == 0u) {
-            uint32_t x, y, z;
-            coords(p, n, x, y, z);
-            const Nb nb = make_nb(p, x, y, z);
-            R f[19];
-            load_prev_out<S, Q>(p, n, nb, f);
-            double s = 0;
+        if ((fg & 3u) != 0u) continue;
+        uint32_t x, y, z;
+        coords(p, n, x, y, z);
+        const Nb nb = make_nb(p, x, y, z);
+        R f[19];
+        load_prev_out<S, Q>(p, n, nb, f);
+        double sum = 0;
 #pragma unroll
-            for (int i = 0; i < 19; i++) s += (double)f[i];
-            const double rho = 1.0 + s;
-            if (isfinite(rho)) v = rho; else nb_bad = 1;
-        }
+        for (int i = 0; i < 19; i++) sum += (double)f[i];
+        const double rho = 1.0 + sum;
+        if (isfinite(rho)) v += rho;
+        else nbad += 1.0;
     }
-    v = warp_sum(v);
-    nb_bad = __reduce_add_sync(0xffffffffu, nb_bad);
-    if ((threadIdx.x & 31) == 0) {
-        if (v != 0.0) atomicAdd(mass, v);
-        if (nb_bad) atomicAdd(bad, (unsigned long long)nb_bad);
-    }
+    grid_sum2<BLOCK>(v, nbad, scratch, out);
 }
 
 // ---------------------------------------------------------------- launchers
@@ -1287,19 +1287,21 @@ cudaError_t launch_dump(int storage, const LatParams &p, int q, cudaStream_t st)
     return cudaGetLastError();
 }
 
+uint32_t mass_blocks() { return (uint32_t)(4 * num_sms()); }
+
 template <class S>
-static void mass_s(const LatParams &p, int q, double *mass, unsigned long long *bad, cudaStream_t st) {
-    const unsigned g = blocks_for(p.N);
-    if (q == 0) k_mass<S, 0><<<g, BLOCK, 0, st>>>(p, mass, bad);
-    else k_mass<S, 1><<<g, BLOCK, 0, st>>>(p, mass, bad);
+static void mass_s(const LatParams &p, int q, double *scratch, double *out, cudaStream_t st) {
+    const unsigned g = std::min<unsigned>(mass_blocks(), blocks_for(p.N));
+    if (q == 0) k_mass<S, 0><<<g, BLOCK, 0, st>>>(p, scratch, out);
+    else k_mass<S, 1><<<g, BLOCK, 0, st>>>(p, scratch, out);
 }
 
-cudaError_t launch_mass(int storage, const LatParams &p, int q, double *mass, unsigned long long *bad, cudaStream_t st) {
+cudaError_t launch_mass(int storage, const LatParams &p, int q, double *scratch, double *out, cudaStream_t st) {
     switch (storage) {
-        case 0: mass_s<float>(p, q, mass, bad, st); break;
-        case 1: mass_s<__half>(p, q, mass, bad, st); break;
-        case 2: mass_s<__nv_bfloat16>(p, q, mass, bad, st); break;
-        case 3: mass_s<double>(p, q, mass, bad, st); break;
+        case 0: mass_s<float>(p, q, scratch, out, st); break;
+        case 1: mass_s<__half>(p, q, scratch, out, st); break;
+        case 2: mass_s<__nv_bfloat16>(p, q, scratch, out, st); break;
+        case 3: mass_s<double>(p, q, scratch, out, st); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

@@ -106,7 +106,10 @@ cudaError_t launch27_step(int storage, const LevelParams &p, const StepArgs &a, 
 cudaError_t launch27_ghost(int storage, const LevelParams &p, const StepArgs &a, cudaStream_t st);
 cudaError_t launch27_restrict(int storage, const LevelParams &p, const StepArgs &a, cudaStream_t st);
 cudaError_t launch27_dump(int storage, const LevelParams &p, uint32_t src, cudaStream_t st);
-cudaError_t launch27_mass(int storage, const LevelParams &p, uint32_t src, double *mass, unsigned long long *bad, cudaStream_t st);
+// FP64 mass and non-finite count into out[0], out[1]; scratch: 2 doubles per
+// block of mass27_blocks() blocks, then a u32 ticket that starts at zero
+uint32_t mass27_blocks();
+cudaError_t launch27_mass(int storage, const LevelParams &p, uint32_t src, double *scratch, double *out, cudaStream_t st);
 // FP64 sum of the records' force and moment into out[0..5] (deterministic
 // order: per-block partials, the last block sums them)
 cudaError_t launch27_reduce(const LevelParams &p, int fp64, double *partials, uint32_t *ticket, double *out, cudaStream_t st);

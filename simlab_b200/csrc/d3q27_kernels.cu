@@ -23,10 +23,12 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "d3q27.h"
 #include "spin_math.cuh"
+#include "reduce.cuh"
 
 namespace lbm27 {
 
@@ -666,27 +668,27 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
+// FP64 mass and non-finite count of the plain fluid cells of a level:
+// grid-stride over the cells, then the deterministic grid sum of reduce.cuh
+// (one atomic per block; the same result on every run).  out[0] = mass,
+// out[1] = non-finite count.
 template <class S>
-__global__ void __launch_bounds__(BLK) k27_mass(const __grid_constant__ LevelParams p, uint32_t src, double *mass, unsigned long long *bad) {
+__global__ void __launch_bounds__(BLK) k27_mass(const __grid_constant__ LevelParams p, uint32_t src, double *scratch, double *out) {
     using R = typename Pop<S>::real;
-    const uint32_t n = blockIdx.x * BLK + threadIdx.x;
-    double m = 0;
-    unsigned nb = 0;
-    if (n < p.N && (p.flags[n] & 7u) == 0) {
+    double m = 0, nbad = 0;
+    const uint32_t stride = gridDim.x * BLK;
+#pragma unroll 1
+    for (uint32_t n = blockIdx.x * BLK + threadIdx.x; n < p.N; n += stride) {
+        if ((p.flags[n] & 7u) != 0) continue;
         R f[27];
         own<S>(p, src, n, f);
-        double s = 1.0;
+        double sum = 1.0;
 #pragma unroll
-        for (int i = 0; i < 27; i++) s += (double)f[i];
-        if (isfinite(s)) m = s;
-        else nb = 1;
+        for (int i = 0; i < 27; i++) sum += (double)f[i];
+        if (isfinite(sum)) m += sum;
+        else nbad += 1.0;
     }
-    m = warp_sum(m);
-    nb = __reduce_add_sync(0xffffffffu, nb);
-    if ((threadIdx.x & 31) == 0) {
-        if (m != 0.0) atomicAdd(mass, m);
-        if (nb) atomicAdd(bad, (unsigned long long)nb);
-    }
+    lbm::grid_sum2<BLK>(m, nbad, scratch, out);
 }
 
 // ------------------------------------------------------------ spinning part
@@ -987,10 +989,22 @@ cudaError_t launch27_dump(int storage, const LevelParams &p, uint32_t src, cudaS
     });
 }
 
-cudaError_t launch27_mass(int storage, const LevelParams &p, uint32_t src, double *mass, unsigned long long *bad, cudaStream_t st) {
+uint32_t mass27_blocks() {
+    static int n = 0;
+    if (!n) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+        if (n <= 0) n = 1;
+    }
+    return (uint32_t)(4 * n);
+}
+
+cudaError_t launch27_mass(int storage, const LevelParams &p, uint32_t src, double *scratch, double *out, cudaStream_t st) {
     return dispatch(storage, [&](auto *t) {
         using S = std::remove_pointer_t<decltype(t)>;
-        k27_mass<S><<<blocks_for(p.N), BLK, 0, st>>>(p, src, mass, bad);
+        const unsigned g = std::min<unsigned>(mass27_blocks(), blocks_for(p.N));
+        k27_mass<S><<<g, BLK, 0, st>>>(p, src, scratch, out);
         return cudaGetLastError();
     });
 }

@@ -824,18 +824,18 @@ int lbm_get_info(const lbm_lattice *h, lbm_info *out) {
 int lbm_mass(lbm_lattice *h, double *mass, uint64_t *nonfinite) {
     if (!h) return LBM_ERR_INVALID;
     return guard(h, [&] {
+        // out[2], then the block partials and the ticket of the grid sum
+        const size_t nb = lbm::mass_blocks();
         double *dm = nullptr;
-        ck(cudaMallocAsync((void **)&dm, 16, h->stream), "cudaMallocAsync");
-        ck(cudaMemsetAsync(dm, 0, 16, h->stream), "memset");
-        ck(lbm::launch_mass(h->setup.storage, h->lp, 1 - h->parity(), dm, (unsigned long long *)(dm + 1), h->stream), "mass kernel");
+        ck(cudaMallocAsync((void **)&dm, (2 + 2 * nb) * sizeof(double) + 16, h->stream), "cudaMallocAsync");
+        ck(cudaMemsetAsync(dm, 0, (2 + 2 * nb) * sizeof(double) + 16, h->stream), "memset");
+        ck(lbm::launch_mass(h->setup.storage, h->lp, 1 - h->parity(), dm + 2, dm, h->stream), "mass kernel");
         double hv[2];
         ck(cudaMemcpyAsync(hv, dm, 16, cudaMemcpyDeviceToHost, h->stream), "mass readback");
         ck(cudaFreeAsync(dm, h->stream), "cudaFreeAsync");
         h->wait();
         if (mass) *mass = hv[0];
-        uint64_t bad;
-        std::memcpy(&bad, &hv[1], 8);
-        if (nonfinite) *nonfinite = bad;
+        if (nonfinite) *nonfinite = (uint64_t)hv[1];
     });
 }
 

@@ -85,8 +85,7 @@ struct lbm_multi {
     uint32_t *ticket = nullptr;
     double *hist = nullptr;       // HIST_CAP x 8 doubles
     double *hist_host = nullptr;  // pinned
-    double *mass_d = nullptr;
-    unsigned long long *bad_d = nullptr;
+    double *mass_d = nullptr;   // mass, non-finite count, then the grid sum's block partials and ticket
     float4 *dump = nullptr;
     uint64_t fine_steps = 0;
     double timeout_s = 600.0;
@@ -478,8 +477,8 @@ void create_multi(const lbm_multi_setup *setup, const lbm_geometry *geom, const 
     h->hist = (double *)h->dalloc(HIST_CAP * 8 * 8);
     ck(cudaMemsetAsync(h->hist, 0, HIST_CAP * 8 * 8, h->stream), "history init");
     ck(cudaMallocHost(&h->hist_host, HIST_CAP * 8 * 8), "cudaMallocHost");
-    h->mass_d = (double *)h->dalloc(16);
-    h->bad_d = (unsigned long long *)h->dalloc(16);
+    h->mass_d = (double *)h->dalloc((2 + 2 * (size_t)lbm27::mass27_blocks()) * sizeof(double) + 16);
+    ck(cudaMemset(h->mass_d, 0, (2 + 2 * (size_t)lbm27::mass27_blocks()) * sizeof(double) + 16), "memset");
     if (s.debug_dump) h->dump = (float4 *)h->dalloc(max_n * sizeof(float4));
     if (spin) {
         lbm27::LevelParams &p = h->lv[finest].p;
@@ -631,14 +630,12 @@ int lbm_multi_mass(lbm_multi *h, uint32_t level, double *mass, uint64_t *nonfini
         if (!mass || !nonfinite) throw MErr(LBM_ERR_INVALID, "null output");
         if (level >= h->lv.size()) throw MErr(LBM_ERR_INVALID, "no such level");
         const Level &L = h->lv[level];
-        ck(cudaMemsetAsync(h->mass_d, 0, 8, h->stream), "mass");
-        ck(cudaMemsetAsync(h->bad_d, 0, 8, h->stream), "mass");
-        ck(lbm27::launch27_mass(h->storage, L.p, L.src, h->mass_d, h->bad_d, h->stream), "mass kernel");
-        unsigned long long bad = 0;
-        ck(cudaMemcpyAsync(mass, h->mass_d, 8, cudaMemcpyDeviceToHost, h->stream), "mass readback");
-        ck(cudaMemcpyAsync(&bad, h->bad_d, 8, cudaMemcpyDeviceToHost, h->stream), "mass readback");
+        ck(lbm27::launch27_mass(h->storage, L.p, L.src, h->mass_d + 2, h->mass_d, h->stream), "mass kernel");
+        double hv[2];
+        ck(cudaMemcpyAsync(hv, h->mass_d, 16, cudaMemcpyDeviceToHost, h->stream), "mass readback");
         h->wait();
-        *nonfinite = bad;
+        *mass = hv[0];
+        *nonfinite = (uint64_t)hv[1];
     });
 }
 
