@@ -341,7 +341,9 @@ typedef struct lbm_multi lbm_multi;
  * finest level's cell indices; wall records use D3Q27 directions
  * (i = (cx+1) + 3 (cy+1) + 9 (cz+1)).  Same validation messages as the
  * reference ("refinement box 1 does not fit inside its parent", "periodic
- * faces only work without refinement", ...).  probes may be NULL. */
+ * faces only work without refinement", ...).  probes (`MProbes`,
+ * mlattice.rs:79-84) may be NULL: vertices relative to `center` in body
+ * coordinates, slices in finest-level cells. */
 int lbm_create_multi(const lbm_multi_setup *setup, const lbm_geometry *geom, const lbm_probes *probes, lbm_multi **out);
 void lbm_multi_destroy(lbm_multi *h);
 int lbm_multi_last_error(const lbm_multi *h, char *buf, uint64_t len);
@@ -373,8 +375,20 @@ int lbm_multi_macros(lbm_multi *h, uint32_t level, float *out);
  * (mask, cell, q as 13 f16 pairs in slot order, force, moment, 3 zero). */
 int lbm_multi_records(lbm_multi *h, uint32_t *out, uint64_t cap_words);
 
-/* steps_done counts finest steps; nrec, memory_bytes, storage as lbm_info;
- * cells = the sum of the levels' cells. */
+/* MultiLattice::reset_samples / vertex_means / slice_means
+ * (mlattice.rs:844-881).  Surface vertices are sampled on the finest level
+ * (trilinear density around each vertex, rotated by the step's StepIn::rot),
+ * each slice pixel (slice coordinates in finest-level cells) on the finest
+ * level whose interior, without its ghost layer, holds it
+ * (mlattice.rs:266-305); both after every finest step whose StepIn::sample is
+ * set.  vertex_means: nvert floats (NaN where nothing was sampled);
+ * slice_means: 4 floats (rho, ux, uy, uz) per pixel. */
+int lbm_multi_reset_samples(lbm_multi *h);
+int lbm_multi_vertex_means(lbm_multi *h, float *out);
+int lbm_multi_slice_means(lbm_multi *h, float *out);
+
+/* steps_done counts finest steps; nrec, memory_bytes, storage, nvert, npix
+ * as lbm_info; cells = the sum of the levels' cells. */
 int lbm_multi_get_info(const lbm_multi *h, lbm_info *out);
 
 /* FP64 mass and non-finite count over the plain fluid cells of one level

@@ -161,13 +161,20 @@ class OracleMulti:
 
     real64=False: the reference's FP32 update; real64=True: the FP64 oracle."""
 
-    def __init__(self, setup, geometry=None, real64: bool = False):
-        from simlab_b200.lbm import geometry_struct
+    def __init__(self, setup, geometry=None, real64: bool = False, probes=None):
+        from simlab_b200.lbm import geometry_struct, probes_struct
 
         L = library()
         vp, u64 = C.c_void_p, C.c_ulonglong
-        L.m27_create.argtypes = [vp, vp, C.c_int]
-        L.m27_create.restype = vp
+        L.m27_create_probes.argtypes = [vp, vp, vp, C.c_int]
+        L.m27_create_probes.restype = vp
+        L.m27_reset_samples.argtypes = [vp]
+        L.m27_vertex_means.argtypes = [vp, vp]
+        L.m27_slice_means.argtypes = [vp, vp]
+        L.m27_nvert.argtypes = [vp]
+        L.m27_nvert.restype = C.c_uint
+        L.m27_npix.argtypes = [vp]
+        L.m27_npix.restype = C.c_uint
         L.m27_destroy.argtypes = [vp]
         L.m27_destroy.restype = None
         L.m27_run.argtypes = [vp, vp, u64, vp]
@@ -185,8 +192,9 @@ class OracleMulti:
         self.setup = setup
         cs, keep = setup.to_c()
         g, keep2 = geometry_struct(geometry)
-        h = L.m27_create(C.addressof(cs), C.addressof(g), int(real64))
-        del keep, keep2
+        pr, keep3 = probes_struct(probes)
+        h = L.m27_create_probes(C.addressof(cs), C.addressof(g), C.addressof(pr) if pr is not None else None, int(real64))
+        del keep, keep2, keep3
         if not h:
             buf = C.create_string_buffer(1024)
             L.orc_last_error(buf, 1024)
@@ -252,6 +260,21 @@ class OracleMulti:
         out = np.zeros(d[0] * d[1] * d[2], dtype=np.uint32)
         self._L.m27_flags(self._h, int(level), out.ctypes.data)
         return out
+
+    def reset_samples(self) -> None:
+        self._L.m27_reset_samples(self._h)
+
+    def vertex_means(self) -> np.ndarray:
+        n = int(self._L.m27_nvert(self._h))
+        out = np.empty(max(n, 1), dtype=np.float32)
+        self._L.m27_vertex_means(self._h, out.ctypes.data)
+        return out[:n]
+
+    def slice_means(self) -> np.ndarray:
+        n = int(self._L.m27_npix(self._h))
+        out = np.empty((max(n, 1), 4), dtype=np.float32)
+        self._L.m27_slice_means(self._h, out.ctypes.data)
+        return out[:n]
 
 
 class OracleGray:

@@ -118,6 +118,14 @@ struct Multi27 {
     uint32_t nrec = 0;
     uint64_t fine_steps = 0;
     Real W[27]{}, W45[27]{};
+    // probes (mlattice.rs:79-84, 243-305): surface vertices on the finest
+    // level, each slice pixel on the finest level whose interior holds it
+    std::vector<std::array<float, 8>> pverts;  // position, 0, normal, 0 (body coordinates)
+    float VOFF = 0.f;
+    std::vector<double> vacc;                  // 2 per vertex: sum of rho, count
+    std::vector<std::vector<std::pair<uint32_t, uint32_t>>> pix;  // per level: (pixel, cell)
+    uint32_t npix = 0;
+    std::vector<double> sacc;                  // 5 per pixel
 
     // ------------------------------------------------------------ storage
     inline Real L(const Level &l, uint32_t set, int d, uint64_t cell) const {
@@ -322,7 +330,7 @@ struct Multi27 {
 
     // ------------------------------------------------------------ setup
     // mlattice.rs:195-548 (host side of MultiLattice::new)
-    void create(const Set &s, const lbm_geometry *geom) {
+    void create(const Set &s, const lbm_geometry *geom, const lbm_probes *probes = nullptr) {
         storage = s.storage;
         ABS_U = s.absorb_velocity != 0;
         TOTAL_P = s.total_pressure_inlet != 0;
@@ -358,6 +366,46 @@ struct Multi27 {
             scale[l] = scale[l - 1] / 2.0;
             for (int k = 0; k < 3; k++) org[l][k] = org[l - 1][k] + s.boxes[l - 1].lo[k] * scale[l - 1];
         }
+        // probes (mlattice.rs:243-305): a slice pixel belongs to the finest
+        // level whose interior without the ghost layer (x in [1, d-2] on the
+        // coarsest level, [2, d-3] on the others) holds its nearest node
+        pix.assign(nl, {});
+        if (probes) {
+            for (uint64_t v = 0; v < probes->nvert; v++) {
+                const double *q = probes->verts + 6 * v;
+                pverts.push_back({(float)q[0], (float)q[1], (float)q[2], 0.f, (float)q[3], (float)q[4], (float)q[5], 0.f});
+            }
+            VOFF = (float)probes->vertex_offset;
+            uint32_t base = 0;
+            for (uint64_t sl = 0; sl < probes->nslices; sl++) {
+                const lbm_slice_def &d = probes->slices[sl];
+                for (uint32_t iv = 0; iv < d.nv; iv++)
+                    for (uint32_t iu = 0; iu < d.nu; iu++) {
+                        const double p[3] = {(double)(d.origin[0] + (int32_t)iu * d.u[0] + (int32_t)iv * d.v[0]),
+                                             (double)(d.origin[1] + (int32_t)iu * d.u[1] + (int32_t)iv * d.v[1]),
+                                             (double)(d.origin[2] + (int32_t)iu * d.u[2] + (int32_t)iv * d.v[2])};
+                        for (size_t l = nl; l-- > 0;) {
+                            const auto dl = dims(l);
+                            const double lo = l == 0 ? 1.0 : 2.0;
+                            bool ok = true;
+                            uint32_t cell[3] = {0, 0, 0};
+                            for (int k = 0; k < 3; k++) {
+                                const double x = std::round((p[k] - org[l][k]) / scale[l]);
+                                if (x < lo || x > (double)dl[k] - 1.0 - lo) { ok = false; break; }
+                                cell[k] = (uint32_t)x;
+                            }
+                            if (ok) {
+                                pix[l].push_back({base + iv * d.nu + iu, (cell[2] * dl[1] + cell[1]) * dl[0] + cell[0]});
+                                break;
+                            }
+                        }
+                    }
+                base += d.nu * d.nv;
+            }
+            npix = base;
+        }
+        vacc.assign(2 * pverts.size(), 0.0);
+        sacc.assign(5 * (size_t)npix, 0.0);
         // records (mlattice.rs:178-192, 345-354); a spinning part makes every
         // swept-box cell of the finest level a record without links
         std::vector<std::pair<uint32_t, uint32_t>> rec_of;
@@ -929,6 +977,7 @@ struct Multi27 {
         lv[l].steps++;
         if (l == finest) {
             out.push_back(reduce());
+            if (sin->sample) sample(base);  // mlattice.rs:812-824
             fine_i++;
         }
         if (l + 1 < nl) {
@@ -948,6 +997,73 @@ struct Multi27 {
             r.src = lv[l].src;
             r.seed = seed_of(0, r.src, 0);
             restrict_fill(l, r);
+        }
+    }
+
+    // mshader.rs:495-505: density and velocity of any cell but a solid one,
+    // from the level's current source set
+    bool cell_macro(const Level &l, uint32_t m, float &rho, float &ux, float &uy, float &uz) const {
+        if ((l.flags[m] & 7u) == q27::T_SOLID) return false;
+        const Mom mo = moments(own(l, l.src, m));
+        const Real r = (Real)1 + mo.rho1;
+        rho = (float)r;
+        ux = (float)(mo.j[0] / r - (Real)0.5 * l.GRAV[0]);
+        uy = (float)(mo.j[1] / r - (Real)0.5 * l.GRAV[1]);
+        uz = (float)(mo.j[2] / r - (Real)0.5 * l.GRAV[2]);
+        return true;
+    }
+
+    // mshader.rs:563-602, after a finest step that asked for samples: the
+    // vertices on the finest level with the step's rotation (trilinear
+    // density over the usable cells around each), then every level's pixels
+    void sample(const Par &par) {
+        const Level &f = lv.back();
+        for (size_t v = 0; v < pverts.size(); v++) {
+            const auto &q = pverts[v];
+            const float b[3] = {q[0] + VOFF * q[4], q[1] + VOFF * q[5], q[2] + VOFF * q[6]};
+            float sp[3], b0[3], fr[3];
+            for (int c = 0; c < 3; c++) {
+                sp[c] = (float)f.CENTER[c] + (par.rot[3 * c] * b[0] + par.rot[3 * c + 1] * b[1] + par.rot[3 * c + 2] * b[2]);
+                b0[c] = std::floor(sp[c]);
+                fr[c] = sp[c] - b0[c];
+            }
+            float acc = 0.f, wsum = 0.f;
+            for (int k = 0; k < 8; k++) {
+                const int o[3] = {k & 1, (k >> 1) & 1, (k >> 2) & 1};
+                const int ci[3] = {(int)b0[0] + o[0], (int)b0[1] + o[1], (int)b0[2] + o[2]};
+                if (ci[0] < 1 || ci[1] < 1 || ci[2] < 1 || ci[0] >= (int)f.NX - 1 || ci[1] >= (int)f.NY - 1 || ci[2] >= (int)f.NZ - 1) continue;
+                const float w = (o[0] ? fr[0] : 1.f - fr[0]) * (o[1] ? fr[1] : 1.f - fr[1]) * (o[2] ? fr[2] : 1.f - fr[2]);
+                float rho, ux, uy, uz;
+                if (cell_macro(f, ((uint32_t)ci[2] * f.NY + (uint32_t)ci[1]) * f.NX + (uint32_t)ci[0], rho, ux, uy, uz) && w > 0.f) {
+                    acc += w * rho;
+                    wsum += w;
+                }
+            }
+            if (wsum > 1e-6f) {
+                vacc[2 * v] += (double)(acc / wsum);
+                vacc[2 * v + 1] += 1.0;
+            }
+        }
+        for (size_t li = 0; li < lv.size(); li++)
+            for (const auto &pc : pix[li]) {
+                float rho, ux, uy, uz;
+                if (cell_macro(lv[li], pc.second, rho, ux, uy, uz)) {
+                    double *a = &sacc[5 * (size_t)pc.first];
+                    a[0] += rho; a[1] += ux; a[2] += uy; a[3] += uz; a[4] += 1.0;
+                }
+            }
+    }
+    void reset_samples() {
+        std::fill(vacc.begin(), vacc.end(), 0.0);
+        std::fill(sacc.begin(), sacc.end(), 0.0);
+    }
+    void vertex_means(float *out) const {
+        for (size_t v = 0; v < pverts.size(); v++) out[v] = vacc[2 * v + 1] > 0 ? (float)(vacc[2 * v] / vacc[2 * v + 1]) : std::nanf("");
+    }
+    void slice_means(float *out) const {
+        for (uint32_t i = 0; i < npix; i++) {
+            const double c = sacc[5 * (size_t)i + 4];
+            for (int a = 0; a < 4; a++) out[4 * i + a] = c > 0 ? (float)(sacc[5 * (size_t)i + a] / c) : std::nanf("");
         }
     }
 

@@ -192,12 +192,12 @@ uint16_t orc_f32_to_bf16(float x) { return oracle::f32_to_bf16(x); }
 float orc_sround16(float x, uint32_t key, uint32_t seed) { return oracle::sround16(x, key, seed); }
 
 
-void *m27_create(const lbm_multi_setup *st, const lbm_geometry *geom, int real64) {
+void *m27_create_probes(const lbm_multi_setup *st, const lbm_geometry *geom, const lbm_probes *probes, int real64) {
     Multi *h = new Multi();
     h->real64 = real64;
     try {
-        if (real64) { h->f64 = new oracle::Multi27<double>(); h->f64->create(*st, geom); }
-        else { h->f32 = new oracle::Multi27<float>(); h->f32->create(*st, geom); }
+        if (real64) { h->f64 = new oracle::Multi27<double>(); h->f64->create(*st, geom, probes); }
+        else { h->f32 = new oracle::Multi27<float>(); h->f32->create(*st, geom, probes); }
         return h;
     } catch (const std::exception &e) {
         g_err = e.what();
@@ -207,6 +207,12 @@ void *m27_create(const lbm_multi_setup *st, const lbm_geometry *geom, int real64
         return nullptr;
     }
 }
+void *m27_create(const lbm_multi_setup *st, const lbm_geometry *geom, int real64) { return m27_create_probes(st, geom, nullptr, real64); }
+int m27_reset_samples(void *hp) { return with(hp, [](auto &m) { m.reset_samples(); return 0; }); }
+int m27_vertex_means(void *hp, float *out) { return with(hp, [&](auto &m) { m.vertex_means(out); return 0; }); }
+int m27_slice_means(void *hp, float *out) { return with(hp, [&](auto &m) { m.slice_means(out); return 0; }); }
+unsigned m27_nvert(void *hp) { return with(hp, [](auto &m) { return (unsigned)m.pverts.size(); }); }
+unsigned m27_npix(void *hp) { return with(hp, [](auto &m) { return (unsigned)m.npix; }); }
 
 void m27_destroy(void *hp) {
     Multi *h = (Multi *)hp;

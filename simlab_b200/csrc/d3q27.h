@@ -106,6 +106,13 @@ cudaError_t launch27_step(int storage, const LevelParams &p, const StepArgs &a, 
 cudaError_t launch27_ghost(int storage, const LevelParams &p, const StepArgs &a, cudaStream_t st);
 cudaError_t launch27_restrict(int storage, const LevelParams &p, const StepArgs &a, cudaStream_t st);
 cudaError_t launch27_dump(int storage, const LevelParams &p, uint32_t src, cudaStream_t st);
+// probes (mshader.rs:563-602): surface vertices on the finest level with the
+// step's rotation, and the (pixel, cell) pairs of the slice pixels a level
+// owns; FP64 running sums in vacc (2 per vertex) and sacc (5 per pixel)
+cudaError_t launch27_sample_verts(int storage, const LevelParams &p, const StepArgs &a, const float *verts, uint32_t nvert, float voff,
+                                  double *vacc, cudaStream_t st);
+cudaError_t launch27_sample_slices(int storage, const LevelParams &p, uint32_t src, const uint32_t *pix, uint32_t npix, double *sacc,
+                                   cudaStream_t st);
 // FP64 mass and non-finite count into out[0], out[1]; scratch: 2 doubles per
 // block of mass27_blocks() blocks, then a u32 ticket that starts at zero
 uint32_t mass27_blocks();

@@ -662,6 +662,71 @@ __global__ void __launch_bounds__(BLK) k27_dump(const __grid_constant__ LevelPar
                             (float)(mo.j[2] / rho - (R)0.5 * k.grav[2]));
 }
 
+// Density and velocity of a cell of a level between steps, from its current
+// source set (mshader.rs:495-505): every cell type but solid has them.
+template <class S>
+__device__ __forceinline__ bool cell_macro27(const LevelParams &p, uint32_t src, uint32_t n, float &rho, float &ux, float &uy, float &uz) {
+    using R = typename Pop<S>::real;
+    if ((p.flags[n] & 7u) == T_SOLID) return false;
+    const Consts27<R> &k = K<R>(p);
+    R f[27];
+    own<S>(p, src, n, f);
+    const Mom<R> mo = moments<R>(f);
+    const R r = (R)1 + mo.rho1;
+    rho = (float)r;
+    ux = (float)(mo.j[0] / r - (R)0.5 * k.grav[0]);
+    uy = (float)(mo.j[1] / r - (R)0.5 * k.grav[1]);
+    uz = (float)(mo.j[2] / r - (R)0.5 * k.grav[2]);
+    return true;
+}
+
+// Surface-pressure probes on the finest level (mshader.rs:563-588): each
+// vertex (body coordinates relative to the centre, pushed out along its
+// normal by voff) rotated by the step's rotation, the density trilinearly
+// interpolated from the usable cells around it; FP64 running sums.
+template <class S>
+__global__ void __launch_bounds__(BLK) k27_sample_verts(const __grid_constant__ LevelParams p, const __grid_constant__ StepArgs a,
+                                                        const float *verts, uint32_t nvert, float voff, double *vacc) {
+    const uint32_t v = blockIdx.x * BLK + threadIdx.x;
+    if (v >= nvert) return;
+    const float bx = verts[8 * v] + voff * verts[8 * v + 4];
+    const float by = verts[8 * v + 1] + voff * verts[8 * v + 5];
+    const float bz = verts[8 * v + 2] + voff * verts[8 * v + 6];
+    float sp[3];
+    for (int c = 0; c < 3; c++) sp[c] = p.kf.center[c] + (a.rot[c * 3] * bx + a.rot[c * 3 + 1] * by + a.rot[c * 3 + 2] * bz);
+    const float b0[3] = {floorf(sp[0]), floorf(sp[1]), floorf(sp[2])};
+    const float fr[3] = {sp[0] - b0[0], sp[1] - b0[1], sp[2] - b0[2]};
+    float acc = 0.f, wsum = 0.f;
+    for (int c = 0; c < 8; c++) {
+        const int o[3] = {c & 1, (c >> 1) & 1, (c >> 2) & 1};
+        const int ci[3] = {(int)b0[0] + o[0], (int)b0[1] + o[1], (int)b0[2] + o[2]};
+        if (ci[0] < 1 || ci[1] < 1 || ci[2] < 1 || ci[0] >= (int)p.NX - 1 || ci[1] >= (int)p.NY - 1 || ci[2] >= (int)p.NZ - 1) continue;
+        const float w = (o[0] ? fr[0] : 1.f - fr[0]) * (o[1] ? fr[1] : 1.f - fr[1]) * (o[2] ? fr[2] : 1.f - fr[2]);
+        float rho, ux, uy, uz;
+        const uint32_t m = ((uint32_t)ci[2] * p.NY + (uint32_t)ci[1]) * p.NX + (uint32_t)ci[0];
+        if (cell_macro27<S>(p, a.src, m, rho, ux, uy, uz) && w > 0.f) { acc += w * rho; wsum += w; }
+    }
+    if (wsum > 1e-6f) {
+        vacc[2 * v] += (double)(acc / wsum);
+        vacc[2 * v + 1] += 1.0;
+    }
+}
+
+// Slice pixels this level owns (mshader.rs:590-602): pairs (pixel, cell),
+// running FP64 sums of (rho, u) and a count per pixel.
+template <class S>
+__global__ void __launch_bounds__(BLK) k27_sample_slices(const __grid_constant__ LevelParams p, uint32_t src, const uint32_t *pix, uint32_t npix,
+                                                         double *sacc) {
+    const uint32_t k = blockIdx.x * BLK + threadIdx.x;
+    if (k >= npix) return;
+    const uint32_t px = pix[2 * k], cell = pix[2 * k + 1];
+    float rho, ux, uy, uz;
+    if (cell_macro27<S>(p, src, cell, rho, ux, uy, uz)) {
+        double *b = sacc + 5ull * px;
+        b[0] += rho; b[1] += ux; b[2] += uy; b[3] += uz; b[4] += 1.0;
+    }
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -985,6 +1050,26 @@ cudaError_t launch27_dump(int storage, const LevelParams &p, uint32_t src, cudaS
     return dispatch(storage, [&](auto *t) {
         using S = std::remove_pointer_t<decltype(t)>;
         k27_dump<S><<<blocks_for(p.N), BLK, 0, st>>>(p, src);
+        return cudaGetLastError();
+    });
+}
+
+cudaError_t launch27_sample_verts(int storage, const LevelParams &p, const StepArgs &a, const float *verts, uint32_t nvert, float voff,
+                                  double *vacc, cudaStream_t st) {
+    if (!nvert) return cudaSuccess;
+    return dispatch(storage, [&](auto *t) {
+        using S = std::remove_pointer_t<decltype(t)>;
+        k27_sample_verts<S><<<blocks_for(nvert), BLK, 0, st>>>(p, a, verts, nvert, voff, vacc);
+        return cudaGetLastError();
+    });
+}
+
+cudaError_t launch27_sample_slices(int storage, const LevelParams &p, uint32_t src, const uint32_t *pix, uint32_t npix, double *sacc,
+                                   cudaStream_t st) {
+    if (!npix) return cudaSuccess;
+    return dispatch(storage, [&](auto *t) {
+        using S = std::remove_pointer_t<decltype(t)>;
+        k27_sample_slices<S><<<blocks_for(npix), BLK, 0, st>>>(p, src, pix, npix, sacc);
         return cudaGetLastError();
     });
 }

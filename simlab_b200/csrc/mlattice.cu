@@ -87,6 +87,15 @@ struct lbm_multi {
     double *hist_host = nullptr;  // pinned
     double *mass_d = nullptr;   // mass, non-finite count, then the grid sum's block partials and ticket
     float4 *dump = nullptr;
+    // probes (mlattice.rs:243-305): surface vertices sampled on the finest
+    // level, slice pixels each taken from the finest level that covers it
+    uint32_t nvert = 0, npix = 0;
+    float voff = 0.f;
+    float *verts = nullptr;               // 8 floats per vertex (position, 0, normal, 0)
+    double *vacc = nullptr;               // 2 doubles per vertex: sum of rho, count
+    double *sacc = nullptr;               // 5 doubles per pixel: sums of rho, u, count
+    std::vector<uint32_t *> pix;          // per level: (pixel, cell) pairs
+    std::vector<uint32_t> npix_l;         // per level: number of pairs
     uint64_t fine_steps = 0;
     double timeout_s = 600.0;
     std::string err;
@@ -151,6 +160,15 @@ struct lbm_multi {
         L.steps++;
         if (l == finest) {
             ck(lbm27::launch27_reduce(L.p, storage == LBM_STORAGE_FP64, partials, ticket, hist + (fine_i % HIST_CAP) * 8, stream), "reduce kernel");
+            if (fine && fine[fine_i].sample) {
+                // mlattice.rs:812-824: vertices with this step's rotation on the
+                // finest level's new state, then the slices of every level
+                lbm27::StepArgs after = a;
+                after.src = L.src;
+                ck(lbm27::launch27_sample_verts(storage, L.p, after, verts, nvert, voff, vacc, stream), "vertex probes");
+                for (size_t q = 0; q < nl; q++)
+                    ck(lbm27::launch27_sample_slices(storage, lv[q].p, lv[q].src, pix[q], npix_l[q], sacc, stream), "slice probes");
+            }
             fine_i++;
         }
         if (l + 1 < nl) {
@@ -266,8 +284,6 @@ void create_multi(const lbm_multi_setup *setup, const lbm_geometry *geom, const 
         per0[a] = p0;
     }
     if (geom && (geom->kind < 0 || geom->kind > 2)) throw MErr(LBM_ERR_INVALID, "unknown geometry kind");
-    if (probes && (probes->nvert || probes->nslices))
-        throw MErr(LBM_ERR_UNSUPPORTED, "vertex and slice probes are not available on the multi-level lattice");
     if (s.dims0[0] < 3 || s.dims0[1] < 3 || s.dims0[2] < 3) throw MErr(LBM_ERR_INVALID, "grid must be at least 3 cells in every direction");
     h->setup = s;
     h->boxes.assign(s.boxes, s.boxes + s.nboxes);
@@ -297,6 +313,52 @@ void create_multi(const lbm_multi_setup *setup, const lbm_geometry *geom, const 
     for (size_t l = 1; l < nl; l++) {
         scale[l] = scale[l - 1] / 2.0;
         for (int k = 0; k < 3; k++) org[l][k] = org[l - 1][k] + h->boxes[l - 1].lo[k] * scale[l - 1];
+    }
+    // probes (mlattice.rs:243-305): each slice pixel (finest-level
+    // coordinates) goes to the finest level whose interior, without its ghost
+    // layer, holds the nearest node
+    std::vector<float> vbuf;
+    std::vector<std::vector<uint32_t>> pix_lists(nl);
+    if (probes) {
+        if (probes->nvert && !probes->verts) throw MErr(LBM_ERR_INVALID, "probe vertices are null");
+        if (probes->nslices && !probes->slices) throw MErr(LBM_ERR_INVALID, "probe slices are null");
+        if (probes->nvert >= 0xffffffffull) throw MErr(LBM_ERR_INVALID, "too many probe vertices");
+        h->nvert = (uint32_t)probes->nvert;
+        h->voff = (float)probes->vertex_offset;
+        for (uint64_t v = 0; v < probes->nvert; v++) {
+            const double *q = probes->verts + 6 * v;
+            const float e[8] = {(float)q[0], (float)q[1], (float)q[2], 0.f, (float)q[3], (float)q[4], (float)q[5], 0.f};
+            vbuf.insert(vbuf.end(), e, e + 8);
+        }
+        uint64_t base = 0;
+        for (uint64_t sl = 0; sl < probes->nslices; sl++) {
+            const lbm_slice_def &d = probes->slices[sl];
+            for (uint32_t iv = 0; iv < d.nv; iv++)
+                for (uint32_t iu = 0; iu < d.nu; iu++) {
+                    const double pt[3] = {(double)(d.origin[0] + (int64_t)iu * d.u[0] + (int64_t)iv * d.v[0]),
+                                          (double)(d.origin[1] + (int64_t)iu * d.u[1] + (int64_t)iv * d.v[1]),
+                                          (double)(d.origin[2] + (int64_t)iu * d.u[2] + (int64_t)iv * d.v[2])};
+                    for (size_t l = nl; l-- > 0;) {
+                        const auto dl = dims(l);
+                        const double lo = l == 0 ? 1.0 : 2.0;
+                        bool ok = true;
+                        uint32_t cell[3];
+                        for (int k = 0; k < 3 && ok; k++) {
+                            const double x = std::round((pt[k] - org[l][k]) / scale[l]);
+                            if (x < lo || x > (double)dl[k] - 1.0 - lo) ok = false;
+                            else cell[k] = (uint32_t)x;
+                        }
+                        if (ok) {
+                            pix_lists[l].push_back((uint32_t)(base + (uint64_t)iv * d.nu + iu));
+                            pix_lists[l].push_back((cell[2] * dl[1] + cell[1]) * dl[0] + cell[0]);
+                            break;
+                        }
+                    }
+                }
+            base += (uint64_t)d.nu * d.nv;
+            if (base >= 0xffffffffull) throw MErr(LBM_ERR_INVALID, "too many slice pixels");
+        }
+        h->npix = (uint32_t)base;
     }
     const auto fd = dims(finest);
     const uint64_t NF = (uint64_t)fd[0] * fd[1] * fd[2];
@@ -476,6 +538,19 @@ void create_multi(const lbm_multi_setup *setup, const lbm_geometry *geom, const 
     ck(cudaMemsetAsync(h->ticket, 0, 16, h->stream), "ticket init");
     h->hist = (double *)h->dalloc(HIST_CAP * 8 * 8);
     ck(cudaMemsetAsync(h->hist, 0, HIST_CAP * 8 * 8, h->stream), "history init");
+    h->verts = (float *)h->dalloc(std::max<size_t>(vbuf.size(), 8) * 4);
+    if (!vbuf.empty()) ck(cudaMemcpyAsync(h->verts, vbuf.data(), vbuf.size() * 4, cudaMemcpyHostToDevice, h->stream), "upload vertices");
+    h->vacc = (double *)h->dalloc(std::max<uint64_t>(h->nvert, 1) * 2 * sizeof(double));
+    h->sacc = (double *)h->dalloc(std::max<uint64_t>(h->npix, 1) * 5 * sizeof(double));
+    ck(cudaMemsetAsync(h->vacc, 0, std::max<uint64_t>(h->nvert, 1) * 2 * sizeof(double), h->stream), "memset");
+    ck(cudaMemsetAsync(h->sacc, 0, std::max<uint64_t>(h->npix, 1) * 5 * sizeof(double), h->stream), "memset");
+    for (size_t l = 0; l < nl; l++) {
+        h->npix_l.push_back((uint32_t)(pix_lists[l].size() / 2));
+        h->pix.push_back((uint32_t *)h->dalloc(std::max<size_t>(pix_lists[l].size(), 2) * 4));
+        if (!pix_lists[l].empty())
+            ck(cudaMemcpyAsync(h->pix[l], pix_lists[l].data(), pix_lists[l].size() * 4, cudaMemcpyHostToDevice, h->stream), "upload pixels");
+    }
+    ck(cudaStreamSynchronize(h->stream), "probe upload");  // host vectors go out of scope
     ck(cudaMallocHost(&h->hist_host, HIST_CAP * 8 * 8), "cudaMallocHost");
     h->mass_d = (double *)h->dalloc((2 + 2 * (size_t)lbm27::mass27_blocks()) * sizeof(double) + 16);
     ck(cudaMemset(h->mass_d, 0, (2 + 2 * (size_t)lbm27::mass27_blocks()) * sizeof(double) + 16), "memset");
@@ -611,12 +686,48 @@ int lbm_multi_records(lbm_multi *h, uint32_t *out, uint64_t cap_words) {
     });
 }
 
+int lbm_multi_reset_samples(lbm_multi *h) {
+    if (!h) return LBM_ERR_INVALID;
+    return mguard(h, [&] {
+        ck(cudaMemsetAsync(h->vacc, 0, std::max<uint64_t>(h->nvert, 1) * 2 * sizeof(double), h->stream), "memset");
+        ck(cudaMemsetAsync(h->sacc, 0, std::max<uint64_t>(h->npix, 1) * 5 * sizeof(double), h->stream), "memset");
+        h->wait();
+    });
+}
+
+int lbm_multi_vertex_means(lbm_multi *h, float *out) {
+    if (!h || (!out && h->nvert)) return LBM_ERR_INVALID;
+    return mguard(h, [&] {
+        if (!h->nvert) return;
+        std::vector<double> v(2 * (size_t)h->nvert);
+        ck(cudaMemcpyAsync(v.data(), h->vacc, v.size() * 8, cudaMemcpyDeviceToHost, h->stream), "vertex readback");
+        h->wait();
+        for (uint32_t i = 0; i < h->nvert; i++) out[i] = v[2 * i + 1] > 0 ? (float)(v[2 * i] / v[2 * i + 1]) : NAN;
+    });
+}
+
+int lbm_multi_slice_means(lbm_multi *h, float *out) {
+    if (!h || (!out && h->npix)) return LBM_ERR_INVALID;
+    return mguard(h, [&] {
+        if (!h->npix) return;
+        std::vector<double> v(5 * (size_t)h->npix);
+        ck(cudaMemcpyAsync(v.data(), h->sacc, v.size() * 8, cudaMemcpyDeviceToHost, h->stream), "slice readback");
+        h->wait();
+        for (uint32_t i = 0; i < h->npix; i++) {
+            const double c = v[5 * i + 4];
+            for (int a = 0; a < 4; a++) out[4 * i + a] = c > 0 ? (float)(v[5 * i + a] / c) : NAN;
+        }
+    });
+}
+
 int lbm_multi_get_info(const lbm_multi *h, lbm_info *out) {
     if (!h || !out) return LBM_ERR_INVALID;
     std::memset(out, 0, sizeof(*out));
     out->steps_done = h->fine_steps;
     out->nrec = h->nrec;
     out->nface = h->lv.empty() ? 0 : h->lv[0].p.nface;
+    out->nvert = h->nvert;
+    out->npix = h->npix;
     out->memory_bytes = h->memory_bytes;
     for (const Level &L : h->lv) out->cells += L.p.N;
     out->storage = h->storage;

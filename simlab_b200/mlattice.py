@@ -14,7 +14,7 @@ from typing import Iterable, Sequence
 
 import numpy as np
 
-from .lbm import (STEP_DTYPE, FaceBc, LbmError, StaticVoxels, StepIn, Storage, _global_error, _Info, _v3, geometry_struct, library,
+from .lbm import (STEP_DTYPE, FaceBc, LbmError, Probes, StaticVoxels, StepIn, Storage, _global_error, _Info, _v3, geometry_struct, library, probes_struct,
                   steps_array)
 
 RS27 = 24  # u32 words per D3Q27 wall record (mshader.rs:32-36)
@@ -141,6 +141,9 @@ def _lib() -> C.CDLL:
         L.lbm_multi_records.argtypes = [vp, C.POINTER(u32), u64]
         L.lbm_multi_get_info.argtypes = [vp, C.POINTER(_Info)]
         L.lbm_multi_mass.argtypes = [vp, u32, dp, C.POINTER(u64)]
+        L.lbm_multi_reset_samples.argtypes = [vp]
+        L.lbm_multi_vertex_means.argtypes = [vp, C.POINTER(C.c_float)]
+        L.lbm_multi_slice_means.argtypes = [vp, C.POINTER(C.c_float)]
         _bound = True
     return L
 
@@ -148,19 +151,22 @@ def _lib() -> C.CDLL:
 class MultiLattice:
     """`MultiLattice` (mlattice.rs:134-906) on one B200.
 
-    MultiLattice(setup, geometry): geometry is None (`MGeometry::None`) or a
-    `StaticVoxels` made with voxelize_static(..., lattice=27) on the finest
-    level (`MGeometry::Static`)."""
+    MultiLattice(setup, geometry, probes): geometry is None (`MGeometry::None`)
+    or a `StaticVoxels` made with voxelize_static(..., lattice=27) on the finest
+    level (`MGeometry::Static`); probes (`MProbes`, mlattice.rs:79-84) a
+    `Probes` of surface vertices relative to the centre and slices in
+    finest-level cells, or None."""
 
-    def __init__(self, setup: MultiSetup, geometry: StaticVoxels | None = None, probes=None):
+    def __init__(self, setup: MultiSetup, geometry: StaticVoxels | None = None, probes: Probes | None = None):
         L = _lib()
         self._L = L
         self.setup = setup
         cs, keep = setup.to_c()
         g, keep2 = geometry_struct(geometry)
+        pr, keep3 = probes_struct(probes)
         h = C.c_void_p()
-        rc = L.lbm_create_multi(C.byref(cs), C.byref(g), None, C.byref(h))
-        del keep, keep2
+        rc = L.lbm_create_multi(C.byref(cs), C.byref(g), C.byref(pr) if pr is not None else None, C.byref(h))
+        del keep, keep2, keep3
         if rc != 0:
             raise _global_error(rc)
         self._h = h
@@ -269,3 +275,28 @@ class MultiLattice:
         bad = C.c_uint64()
         self._check(self._L.lbm_multi_mass(self._h, int(level), C.byref(m), C.byref(bad)))
         return m.value, int(bad.value)
+
+    @property
+    def nvert(self) -> int:
+        return int(self.info().nvert)
+
+    @property
+    def npix(self) -> int:
+        return int(self.info().npix)
+
+    def reset_samples(self) -> None:
+        """MultiLattice::reset_samples (mlattice.rs:844-858)."""
+        self._check(self._L.lbm_multi_reset_samples(self._h))
+
+    def vertex_means(self) -> np.ndarray:
+        """Mean density at each surface vertex over the sampled finest steps
+        (mlattice.rs:860-867); NaN where nothing was sampled."""
+        out = np.empty(max(self.nvert, 1), dtype=np.float32)
+        self._check(self._L.lbm_multi_vertex_means(self._h, out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out[:self.nvert]
+
+    def slice_means(self) -> np.ndarray:
+        """Mean (rho, ux, uy, uz) per slice pixel (mlattice.rs:869-881)."""
+        out = np.empty((max(self.npix, 1), 4), dtype=np.float32)
+        self._check(self._L.lbm_multi_slice_means(self._h, out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out[:self.npix]

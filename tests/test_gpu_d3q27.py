@@ -161,3 +161,44 @@ def test_mass_conserved_with_halfway_walls(storage, tol):
     m1, b1 = g.mass(0)
     assert b0 == 0 and b1 == 0
     assert abs(m1 / m0 - 1.0) < tol
+
+
+def test_three_levels_probes_match_oracle():
+    """Multi-level probes (mlattice.rs:243-305, 844-881; mshader.rs:563-602)
+    against the oracle, FP32: surface vertices of the sphere on the finest
+    level read through a rotated body frame (StepIn::rot; a sphere turned
+    about its centre has the same surface), and two slices whose pixels come
+    from all three levels; sampling after every finest step from step 21 on,
+    the averages over the remaining 40 steps."""
+    from simlab_b200.lbm import Probes, SliceDef
+
+    s, vox = feature_multi()
+    c = np.array(s.center)
+    v, t = sphere(list(c), 3.5, 2)
+    rel = np.asarray(v) - c
+    verts = [(tuple(p), tuple(p / np.linalg.norm(p))) for p in rel]
+    org2 = np.array([4 * 12 + 2 * 8, 4 * 9 + 2 * 7, 4 * 9 + 2 * 7])  # the finest level's node 0 in finest units
+    zc = int(org2[2] + round(c[2]))
+    slices = [SliceDef(origin=[0, 0, zc], u=[3, 0, 0], v=[0, 3, 0], nu=63, nv=47),
+              SliceDef(origin=[int(org2[0]) - 6, int(org2[1]) - 4, zc + 1], u=[1, 0, 0], v=[0, 1, 0], nu=40, nv=30)]
+    probes = Probes(verts=verts, slices=slices, vertex_offset=0.5)
+    g, o = MultiLattice(s, vox, probes=probes), OracleMulti(s, vox, probes=probes)
+    a = spin(60)
+    th = 0.4
+    a["rot"] = np.array([[np.cos(th), -np.sin(th), 0.0], [np.sin(th), np.cos(th), 0.0], [0.0, 0.0, 1.0]])
+    a["sample"][20:] = 1
+    g.run(a[:20]), o.run(a[:20])
+    g.reset_samples(), o.reset_samples()
+    g.run(a[20:]), o.run(a[20:])
+    vg, vo = g.vertex_means(), o.vertex_means()
+    assert len(vg) == len(verts) and np.array_equal(np.isnan(vg), np.isnan(vo))
+    ok = ~np.isnan(vo)
+    assert ok.sum() > 0.9 * len(verts)
+    assert np.max(np.abs(vg[ok] - vo[ok])) < 1e-5
+    sg, so = g.slice_means(), o.slice_means()
+    assert sg.shape == so.shape == (63 * 47 + 40 * 30, 4)
+    assert np.array_equal(np.isnan(sg[:, 0]), np.isnan(so[:, 0]))
+    ok = ~np.isnan(so[:, 0])
+    assert ok.sum() > 0.9 * len(so)
+    assert np.max(np.abs(sg[ok, 0] - so[ok, 0])) < 1e-5
+    assert rel_l2(sg[ok, 1:].astype(np.float64), so[ok, 1:].astype(np.float64)) <= 1e-5

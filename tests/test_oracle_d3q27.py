@@ -105,3 +105,34 @@ def test_oracle_multi_step_count_must_be_a_multiple():
 
     with pytest.raises(RuntimeError, match="multiple of 4"):
         lat.run(3)
+
+
+def test_oracle_probes_uniform_stream_across_levels():
+    """Probes on the refined lattice (mlattice.rs:243-305, 844-881;
+    mshader.rs:563-602): in the uniform stream of refined.rs:100-119 every
+    sampled pixel, whichever level it is taken from, and every surface vertex
+    read the stream's state; pixels on the coarsest level's boundary nodes
+    (outside its interior) have no level and stay NaN."""
+    from simlab_b200.lbm import Probes, SliceDef, steps_array
+
+    s = uniform_refined_setup()
+    fd = s.dims(2)
+    s.center = [0.5 * (fd[0] - 1) + 0.3, 0.5 * (fd[1] - 1) + 0.2, 0.5 * (fd[2] - 1) + 0.1]
+    verts = [((2.0 * np.cos(a), 2.0 * np.sin(a), 0.5), (np.cos(a), np.sin(a), 0.0)) for a in np.linspace(0, 6.0, 7)]
+    slices = [SliceDef(origin=[0, 0, 96], u=[4, 0, 0], v=[0, 4, 0], nu=64, nv=48),     # the whole coarse plane
+              SliceDef(origin=[60, 44, 95], u=[1, 0, 0], v=[0, 1, 0], nu=120, nv=90)]  # across both refinement boxes
+    o = OracleMulti(s, probes=Probes(verts=verts, slices=slices, vertex_offset=0.5))
+    a = steps_array(8)
+    a["sample"] = 1
+    o.run(a)
+    vm = o.vertex_means()
+    assert vm.shape == (7,) and np.all(np.abs(vm - 1.0) < 1e-5)
+    sm = o.slice_means()
+    assert sm.shape == (64 * 48 + 120 * 90, 4)
+    c = sm[:64 * 48].reshape(48, 64, 4)
+    assert np.all(np.isnan(c[:, 0, 0])) and np.all(np.isnan(c[0, :, 0]))  # x = 0, y = 0 coarse boundary nodes
+    ok = ~np.isnan(sm[:, 0])
+    assert ok.sum() >= 62 * 46 + 120 * 90
+    assert np.all(np.abs(sm[ok, 0] - 1.0) < 1e-5) and np.all(np.abs(sm[ok, 1] - 0.06) < 1e-5) and np.all(np.abs(sm[ok, 2:]) < 1e-6)
+    o.reset_samples()
+    assert np.all(np.isnan(o.vertex_means())) and np.all(np.isnan(o.slice_means()[:, 0]))
