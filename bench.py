@@ -412,6 +412,77 @@ def c5_adjoint():
     return out
 
 
+def c3_rotor(steps: int = 256, warmup: int = 32):
+    """C3's workload: the three-level D3Q27 rotor case (simlab_b200.cases.
+    prop_refined: coarse 256x128x128 + 8.1 M + 16.0 M cells, the two-blade
+    rotor of radius 60 finest cells re-voxelized on the finest level every
+    finest step), spinning at full speed; MLUPS by the finest-step definition
+    of tunnel.rs:800-804, device time of `steps` finest steps through
+    lbm_multi_run (force readback included), FP32 and FP16 storage."""
+    import torch
+
+    from simlab_b200.cases import prop_refined, spin_schedule
+    from simlab_b200.lbm import Storage
+    from simlab_b200.mlattice import MultiLattice
+
+    res = {}
+    for storage in (Storage.FP32, Storage.FP16):
+        s, geo, om = prop_refined(storage)
+        g = MultiLattice(s, geo)
+        sched = spin_schedule(warmup + steps, om, 1)
+        g.run(sched[:warmup])
+        stream = torch.cuda.ExternalStream(g.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record()
+        f = g.run(sched[warmup:])
+        with torch.cuda.stream(stream):
+            e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        cells = g.level_cells()
+        lups = sum(c * 2 ** l for l, c in enumerate(cells)) / 2 ** (len(cells) - 1) * steps
+        res[storage.name.lower()] = {"mlups": round(lups / ms / 1e3, 1), "ms_per_finest_step": round(ms / steps, 4),
+                                     "records": int(g.nrec), "finite": bool(np.all(np.isfinite(f)))}
+        g.close()
+    res["cells"] = cells
+    return res
+
+
+def spin_overhead(steps: int = 100, warmup: int = 10):
+    """A spinning part against the same part held still (the reference
+    reports spinning runs taking 2.3x their estimate, crates/engine/src/wind.rs:
+    537-543): the refined case's two-blade rotor (radius 40 cells) on one
+    256x128x128 D3Q19 level, FP16 storage; spinning, every swept-box cell is a
+    record and the GPU re-voxelizes the box every step.  Device time per step
+    of each and their ratio."""
+    import torch
+
+    from simlab_b200.cases import rotor_tunnel, spin_schedule
+    from simlab_b200.lbm import Lattice, Storage
+
+    out = {}
+    for spinning in (False, True):
+        st, geo, om = rotor_tunnel(Storage.FP16, spinning=spinning)
+        lat = Lattice(st, geo)
+        sched = spin_schedule(warmup + steps, om if spinning else 0.0, 1)
+        lat.run(sched[:warmup])
+        stream = torch.cuda.ExternalStream(lat.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record()
+        f = lat.run(sched[warmup:])
+        with torch.cuda.stream(stream):
+            e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        out["spinning" if spinning else "static"] = {"ms_per_step": round(ms / steps, 4), "mlups": round(st.cells() * steps / ms / 1e3, 1),
+                                                     "records": int(lat.nrec), "finite": bool(np.all(np.isfinite(f)))}
+        lat.close()
+    out["spin_over_static"] = round(out["spinning"]["ms_per_step"] / out["static"]["ms_per_step"], 3)
+    return out
+
+
 def run_reference(args, ws, rank):
     """The reference arm: the oracle on the host cores, rank 0 only, on the
     same workload, metric and config as the engine's line; each step one
@@ -513,6 +584,8 @@ def main():
         line["d3q27_three_levels_mlups"] = d3q27_levels()
         line["c5_fp16_1024x512x512"] = c5_throughput()
         line["c5_adjoint"] = c5_adjoint()
+        line["c3_rotor"] = c3_rotor()
+        line["spin_overhead"] = spin_overhead()
     if rank == 0 and ws == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_oracle_sample(budget_s=12.0)[0]
     if rank == 0:

@@ -220,3 +220,28 @@ def prop_gray_band(storage=Storage.FP16, dims=(384, 192, 192), radius=60.0, band
     spec = AdjointSpec(steps=steps, t0=steps // 2 + 1, t1=steps, checkpoint_every=checkpoint_every, objective=1, dir=[1.0, 0.0, 0.0],
                        recompute=False)
     return st, gam, near.reshape(-1), spec
+
+
+# ------------------------------------------------------------------ spinning-part overhead case
+def rotor_tunnel(storage=Storage.FP16, spinning: bool = True, dims=(256, 128, 128), radius=40.0, tip_speed=0.08, u=0.03, nu=4e-4):
+    """One D3Q19 level with the refined case's two-blade rotor (radius 40
+    cells here), axis along the flow, in the reference's wind-tunnel faces:
+    spinning (`Geometry::Spin`: every cell of the swept box a record,
+    re-voxelized each step) or held still (`Geometry::Static` of the same
+    surface at angle zero).  Returns (setup, geometry, omega)."""
+    from .lbm import SpinGeometry, voxelize_spin
+    from .shapes import propeller
+
+    c = [0.5 * (dims[0] - 1) - 32.0 + 0.31, 0.5 * (dims[1] - 1) + 0.23, 0.5 * (dims[2] - 1) + 0.17]
+    F = FaceBc
+    st = LatticeSetup(dims=list(dims), faces=[F.VELOCITY] + [F.OPEN] * 5, nu=nu, u_inf=[u, 0.0, 0.0], u_init=[u, 0.0, 0.0],
+                      storage=storage, center=c, collision=Collision.REGULARIZED, total_pressure_inlet=True)
+    v, t = propeller(radius=radius)
+    if spinning:
+        sv = voxelize_spin(v, t, [0.0, 0.0, 1.0], 0.125)
+        r = int(np.ceil(sv.radius)) + 3
+        lo, hi = int(np.floor(c[0] + sv.axial[0])) - 3, int(np.ceil(c[0] + sv.axial[1])) + 3
+        geo = SpinGeometry(vox=sv, box_lo=[lo, int(c[1]) - r, int(c[2]) - r], box_n=[hi - lo + 1, 2 * r + 2, 2 * r + 2])
+    else:
+        geo = voxelize_static(np.asarray(v, dtype=np.float64) @ BODY_TO_LATTICE.T + np.asarray(c), t, list(dims))
+    return st, geo, tip_speed / radius
