@@ -353,14 +353,82 @@ __device__ __forceinline__ void face_values(const LatParams &p, const Consts<R> 
     for (int i = 0; i < 19; i++) f[i] = feq_i<R>(i, rho1, rho, ux, uy, uz, usq) + fneq_i<R>(i, pi, tr);
 }
 
+// A velocity-inlet or open face cell b of face F whose store mask is the
+// planar one: its five targets and its inner neighbour's 19 sources lie
+// inside the domain without wrapping when the face's two in-plane axes are
+// not periodic, so every offset is a plain stride and the directions are
+// known at compile time.  The same values, rounding sequence and slots as
+// the general path.
+template <class S, int Q, int F>
+__device__ __forceinline__ void face_planar(const LatParams &p, const StepParams &s, uint32_t b, uint32_t info) {
+    using R = typename Pop<S>::real;
+    constexpr int A = F >> 1;
+    constexpr uint32_t MASK = planar_mask(F);
+    const int32_t nx = (int32_t)p.NX, nxy = (int32_t)(p.NX * p.NY);
+    const Nb flat{1, -1, nx, -nx, nxy, -nxy};
+    const int32_t in = (F & 1 ? -1 : 1) * (A == 0 ? 1 : (A == 1 ? nx : nxy));
+    const uint32_t m = (uint32_t)((int32_t)b + in);
+    const bool fluid = (p.flags[m] & 3u) == 0u;
+    R g[19];
+    load_prev_out<S, Q>(p, m, flat, g);
+    const Consts<R> &k = K<R>(p);
+    R rho = 1, ux = k.u_inf[0], uy = k.u_inf[1], uz = k.u_inf[2];
+    R pi[6] = {0, 0, 0, 0, 0, 0};
+    if (fluid) {
+        const Moments<R> mo = moments<R>(g);
+        rho = (R)1 + mo.rho1;
+        ux = mo.jx / rho - (R)0.5 * k.grav[0];
+        uy = mo.jy / rho - (R)0.5 * k.grav[1];
+        uz = mo.jz / rho - (R)0.5 * k.grav[2];
+        pi_neq<R>(mo, rho, ux, uy, uz, pi);
+    }
+    if ((info & 3u) == 0u) {
+        if (p.total_p) {
+            const R uinf2 = k.u_inf[0] * k.u_inf[0] + k.u_inf[1] * k.u_inf[1] + k.u_inf[2] * k.u_inf[2];
+            rho = ((R)(1.0 / 3.0) + (R)0.5 * uinf2) / ((R)(1.0 / 3.0) + (R)0.5 * (ux * ux + uy * uy + uz * uz));
+        } else {
+            ux = k.u_inf[0]; uy = k.u_inf[1]; uz = k.u_inf[2];
+        }
+    } else {
+        rho = 1;
+    }
+    const R rho1 = rho - (R)1;
+    const R usq = (R)1.5 * (ux * ux + uy * uy + uz * uz);
+    const R tr = (pi[0] + pi[1] + pi[2]) * (R)(1.0 / 3.0);
+    Rng rng{sr_hash_mix(b, s.seed_mix)};
+    S *pop = (S *)p.pop;
+    constexpr_for<0, 19>([&](auto I) {
+        constexpr int i = decltype(I)::value;
+        if constexpr ((MASK >> i) & 1u) {
+            const S v = Pop<S>::enc(feq_i<R>(i, rho1, rho, ux, uy, uz, usq) + fneq_i<R>(i, pi, tr), rng);
+            if (Q == 0) pop[(uint64_t)OPP(i) * p.NP + b] = v;
+            else pop[(uint64_t)i * p.NP + (uint32_t)((int32_t)b + flat.off(CX(i), CY(i), CZ(i)))] = v;
+        }
+    });
+}
+
 template <class S, int P>
 __global__ void __launch_bounds__(BLOCK) k_faces(const __grid_constant__ LatParams p, const __grid_constant__ StepParams s) {
     using R = typename Pop<S>::real;
     constexpr int Q = 1 - P;
-    const uint32_t kf = blockIdx.x * BLOCK + threadIdx.x;
-    if (kf >= s.nface) return;
+    // the block's group: planar cells of one face (F < 6), or the rest
+    int F = 6;
+#pragma unroll
+    for (int g = 5; g >= 0; g--)
+        if (blockIdx.x < p.fblk[g + 1]) F = g;
+    const uint32_t kf = p.fplan[F] + (blockIdx.x - p.fblk[F]) * BLOCK + threadIdx.x;
+    if (kf >= (F < 6 ? p.fplan[F + 1] : s.nface)) return;
     const uint32_t b = p.faces[kf];
     const uint32_t info = p.face_info[kf];
+    switch (F) {
+        case 0: face_planar<S, Q, 0>(p, s, b, info); return;
+        case 1: face_planar<S, Q, 1>(p, s, b, info); return;
+        case 2: face_planar<S, Q, 2>(p, s, b, info); return;
+        case 3: face_planar<S, Q, 3>(p, s, b, info); return;
+        case 4: face_planar<S, Q, 4>(p, s, b, info); return;
+        case 5: face_planar<S, Q, 5>(p, s, b, info); return;
+        default: break;
+    }
     uint32_t x, y, z;
     coords(p, b, x, y, z);
     uint32_t cx = x, cy = y, cz = z;
@@ -1220,7 +1288,7 @@ static cudaError_t step_t(const LatParams &p, const StepParams &s, cudaStream_t 
         k_walls<S, P, COLL><<<(unsigned)((p.nrec + WBLOCK - 1) / WBLOCK), WBLOCK, 0, side>>>(p, s);
         cudaEventRecord(join, side);
     }
-    if (s.nface) k_faces<S, P><<<blocks_for(s.nface), BLOCK, 0, st>>>(p, s);
+    if (s.nface) k_faces<S, P><<<p.fblk[6] + blocks_for(s.nface - p.fplan[6]), BLOCK, 0, st>>>(p, s);
     if (ev) cudaEventRecord(ev[1], st);
     if (overlap) cudaStreamWaitEvent(st, join, 0);
     else if (p.nrec) k_walls<S, P, COLL><<<(unsigned)((p.nrec + WBLOCK - 1) / WBLOCK), WBLOCK, 0, st>>>(p, s);

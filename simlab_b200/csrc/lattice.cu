@@ -397,15 +397,37 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
             xinfo[x == 0 ? 0 : 1] = finfo[k] & 0xffu;
         }
     }
+    uint32_t fplan[7] = {0, 0, 0, 0, 0, 0, 0}, fblk[7] = {0, 0, 0, 0, 0, 0, 0};
     {
         // face cells are independent; grouping them by kind and store mask
-        // keeps each warp on one code path
+        // keeps each warp on one code path.  Planar cells of a velocity or
+        // open face whose in-plane axes are not periodic come first, one
+        // group per face: the face kernel handles them with compile-time
+        // directions and plain strides.
+        auto group = [&](size_t k) -> int {
+            const uint32_t info = finfo[k];
+            if (fused[k] || (info & 3u) == 2u) return 6;
+            for (int f = 0; f < 6; f++) {
+                const int a = f >> 1;
+                if ((info >> 8) == lbm::planar_mask(f) && !per[a == 0 ? 1 : 0] && !per[a == 2 ? 1 : 2]) return f;
+            }
+            return 6;
+        };
+        std::vector<int> grp(faces.size());
+        for (size_t k = 0; k < faces.size(); k++) grp[k] = group(k);
         std::vector<size_t> ord(faces.size());
         for (size_t k = 0; k < ord.size(); k++) ord[k] = k;
         std::stable_sort(ord.begin(), ord.end(), [&](size_t a, size_t b) {
             if (fused[a] != fused[b]) return fused[a] < fused[b];
+            if (grp[a] != grp[b]) return grp[a] < grp[b];
             return finfo[a] < finfo[b];
         });
+        uint32_t cnt[7] = {0, 0, 0, 0, 0, 0, 0};
+        for (size_t k = 0; k < faces.size(); k++) cnt[grp[k]]++;
+        for (int f = 1; f < 7; f++) {
+            fplan[f] = fplan[f - 1] + cnt[f - 1];
+            fblk[f] = fblk[f - 1] + (cnt[f - 1] + (uint32_t)lbm::BLOCK - 1) / (uint32_t)lbm::BLOCK;
+        }
         std::vector<uint32_t> f2(faces.size()), i2(faces.size());
         uint32_t rest = 0;
         for (size_t k = 0; k < ord.size(); k++) {
@@ -519,6 +541,7 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     fill_consts<double>(p.kd, st);
     p.xface_info[0] = xinfo[0];
     p.xface_info[1] = xinfo[1];
+    for (int f = 0; f < 7; f++) { p.fplan[f] = fplan[f]; p.fblk[f] = fblk[f]; }
     // sponge ramps per axis (shader.rs:528-538): 1 - p / width inside a layer
     std::vector<float> tabf;
     std::vector<double> tabd;

@@ -36,6 +36,16 @@ __host__ __device__ __forceinline__ constexpr int CZ(int i) {
 }
 __host__ __device__ __forceinline__ constexpr int OPP(int i) { return i == 0 ? 0 : ((i & 1) ? i + 1 : i - 1); }
 __host__ __device__ __forceinline__ constexpr double WD(int i) { return i == 0 ? 1.0 / 3.0 : (i <= 6 ? 1.0 / 18.0 : 1.0 / 36.0); }
+// The store mask of a planar cell of face F (0..5: -x, +x, -y, +y, -z, +z)
+// away from the face's edges: the five directions pointing into the domain.
+__host__ __device__ __forceinline__ constexpr uint32_t planar_mask(int F) {
+    uint32_t m = 0;
+    for (int i = 0; i < 19; i++) {
+        const int c = (F >> 1) == 0 ? CX(i) : ((F >> 1) == 1 ? CY(i) : CZ(i));
+        if (c == ((F & 1) ? -1 : 1)) m |= 1u << i;
+    }
+    return m;
+}
 __host__ __device__ __forceinline__ constexpr int DIR(int x, int y, int z) {
     int r = 0;
     for (int i = 0; i < 19; i++)
@@ -125,6 +135,12 @@ struct LatParams {
     const float *sp_tab;       // sponge ramp per x, then per y, then per z (NX + NY + NZ values)
     const double *sp_tabd;     // the same in FP64
     uint32_t xface_info[2];    // face info (kind | mirror << 2) of the -x and +x faces, for fused x faces
+    // The face list is ordered planar cells of faces 0..5 (velocity or open
+    // faces whose store mask is planar_mask(F), in-plane axes not periodic),
+    // then the rest (edges, corners, free slip), then fused x-face cells.
+    // fplan[F]: first list index of group F (F = 6: the rest); fblk[F]: the
+    // face kernel's first block for group F.
+    uint32_t fplan[7], fblk[7];
     int tma;                   // the staged bulk kernel applies (NX * element size % 16 == 0)
     // spinning part (Geometry::Spin, lattice.rs:87-92): every cell of the swept
     // box is a record, re-voxelized each step from the rotated surface

@@ -6,6 +6,19 @@
     python -m simlab_b200.profile_case d3q27 [fp16|fp32|bf16|fp64] [steps]
         a single-level D3Q27 wind tunnel, 256x128x128 (4.2 M cells; 453 MB of
         FP16 populations in two sets), velocity inlet, open faces, sponges
+    python -m simlab_b200.profile_case levels [fp16|fp32] [finest steps]
+        the refined rotor case on a 128x64x64 coarse level with its two boxes
+        (3.6 M cells; 392 MB of FP16 populations): ghosts, restriction, faces,
+        force reduction and the D3Q27 re-voxelizer of the spinning rotor
+    python -m simlab_b200.profile_case spin [steps]
+        the two-blade rotor (radius 40) spinning on one 256x128x128 D3Q19 level,
+        FP16: the D3Q19 re-voxelizer and moving-wall records
+    python -m simlab_b200.profile_case probes [steps]
+        the arm case on 512x256x64, FP16, with 10,000 surface probes and two
+        slices sampled every step, then the FP64 mass check
+    python -m simlab_b200.profile_case gray [steps]
+        the gray-level design case (192x96x96, FP32): forward steps, then one
+        adjoint sweep over the same steps (checkpoint every 10)
 """
 from __future__ import annotations
 
@@ -23,8 +36,72 @@ def d3q27_tunnel(storage: Storage):
                       sponge=[0, 16, 8, 8, 8, 8], sponge_tau=1.0, sponge_sigma=0.1, total_pressure_inlet=True, storage=storage)
 
 
+def _levels(args) -> None:
+    from .cases import prop_refined, spin_schedule
+    from .mlattice import MultiLattice
+
+    storage = Storage[(args[0] if args else "fp16").upper()]
+    steps = int(args[1]) if len(args) > 1 else 8
+    s, geo, om = prop_refined(storage, radius=30.0, dims0=(128, 64, 64))
+    lat = MultiLattice(s, geo)
+    f = lat.run(spin_schedule(steps, om, 1))
+    print(f"profile case levels {storage.name} {lat.level_cells()}: {steps} finest steps, last force {f[-1][:3]}")
+
+
+def _spin(args) -> None:
+    from .cases import rotor_tunnel, spin_schedule
+
+    steps = int(args[0]) if args else 6
+    st, geo, om = rotor_tunnel(Storage.FP16, spinning=True)
+    lat = Lattice(st, geo)
+    f = lat.run(spin_schedule(steps, om, 1))
+    print(f"profile case spin: {steps} steps, {lat.nrec} records, last force {f[-1][:3]}")
+
+
+def _probes(args) -> None:
+    import numpy as np
+
+    from .lbm import Probes, SliceDef
+
+    steps = int(args[0]) if args else 6
+    st, vox = arm_les(Storage.FP16, dims=(512, 256, 64))
+    rng = np.random.default_rng(7)
+    c = np.asarray(st.center)
+    verts = [(rng.uniform(-20, 20, 3), np.array([1.0, 0.0, 0.0])) for _ in range(10000)]
+    sl = [SliceDef(origin=(1, int(c[1]), 1), u=(1, 0, 0), v=(0, 0, 1), nu=510, nv=62),
+          SliceDef(origin=(int(c[0]), 1, 1), u=(0, 1, 0), v=(0, 0, 1), nu=254, nv=62)]
+    lat = Lattice(st, vox, Probes(verts=verts, slices=sl, vertex_offset=1.0))
+    lat.run(steps_array_sampled(steps))
+    m, bad = lat.mass()
+    print(f"profile case probes: {steps} sampled steps, {lat.npix} pixels, mass {m:.6e}, non-finite {bad}")
+
+
+def steps_array_sampled(n: int):
+    from .lbm import steps_array
+
+    return steps_array(n, sample=True)
+
+
+def _gray(args) -> None:
+    from .cases import gray_design
+    from .gray import AdjointSpec, GrayLattice
+
+    steps = int(args[0]) if args else 20
+    st, gam, _ = gray_design()
+    lat = GrayLattice(st, gam)
+    lat.run(steps)
+    lat.reset()
+    spec = AdjointSpec(steps=steps, t0=steps // 2 + 1, t1=steps, checkpoint_every=10, objective=0, dir=[1.0, 0.0, 0.0], recompute=True)
+    j, g = lat.backward(spec)
+    print(f"profile case gray: {steps} steps forward, adjoint objective {j:.6e}, |grad| {float((g * g).sum()) ** 0.5:.3e}")
+
+
 def main() -> None:
     args = sys.argv[1:]
+    cases = {"levels": _levels, "spin": _spin, "probes": _probes, "gray": _gray}
+    if args and args[0] in cases:
+        cases[args[0]](args[1:])
+        return
     if args and args[0] == "d3q27":
         from .mlattice import MultiLattice
 
