@@ -42,6 +42,31 @@ sys.path.insert(0, str(ROOT))
 METRIC = "MLUPS (D3Q19 LES arm 512x256x256, FP16-stored populations)"
 UNIT = "MLUPS"
 DTYPE = "f32 arithmetic, fp16 storage"
+# Arithmetic per lattice update of the two collision kernels, FP16 storage,
+# from ncu's executed-instruction counts by opcode
+# (profiles/opcode_mix_k_bulk_tma_k27_step_fp16.md): flops = FADD + FMUL +
+# 2 FFMA per cell; instructions = all thread instructions per cell (D3Q19
+# includes the copy pipeline's wait loops).  FP32 peak: 148 SMs x 128 FP32
+# lanes x 2 flops x clock; issue peak: 148 SMs x 4 schedulers x 32 threads x clock.
+ALU_PER_LUP = {"d3q19_bulk_fp16": {"flops": 85.7 + 50.6 + 2 * 71.4, "instr": 580.2},
+               "d3q27_step_fp16": {"flops": 161.5 + 175.0 + 2 * 177.0, "instr": 1012.0}}
+
+
+def alu_line(lups: dict, sm_mhz: float) -> dict:
+    """FP32 throughput and issue rate of the collision kernels from their
+    measured update rates (updates/s) and the per-update counts above."""
+    f = sm_mhz * 1e6
+    peak_fp32, peak_issue = 148 * 128 * 2 * f, 148 * 4 * 32 * f
+    out = {"fp32_peak_tflops": round(peak_fp32 / 1e12, 2), "issue_peak_tinst_s": round(peak_issue / 1e12, 2), "sm_mhz": sm_mhz,
+           "source": "profiles/opcode_mix_k_bulk_tma_k27_step_fp16.md"}
+    for k, ups in lups.items():
+        c = ALU_PER_LUP[k]
+        out[k] = {"flops_per_lup": round(c["flops"], 1), "instr_per_lup": c["instr"], "glups": round(ups / 1e9, 2),
+                  "fp32_tflops": round(c["flops"] * ups / 1e12, 2), "fp32_frac": round(c["flops"] * ups / peak_fp32, 3),
+                  "issue_frac": round(c["instr"] * ups / peak_issue, 3)}
+    return out
+
+
 CONFIG = {"workload": "D3Q19 regularized + Smagorinsky LES (Cs 0.17), arm 200x12x8 + cylinder r10 h14, 512x256x256, "
                       "u 0.05, Re 1e5, Bouzidi walls, wind-tunnel faces + sponges",
           "storage": "fp16 (f - w) x 32768, stochastic rounding",
@@ -300,11 +325,11 @@ def d3q27_levels():
     from simlab_b200.mlattice import LevelBox, MultiLattice, MultiSetup
 
     res = {}
-    for storage in (Storage.FP32, Storage.FP16):
+    for storage, nl in ((Storage.FP32, 3), (Storage.FP16, 3), (Storage.FP16, 1)):
         F = FaceBc
         s = MultiSetup(dims0=[256, 128, 128], faces=[F.VELOCITY] + [F.OPEN] * 5, nu0=0.001, u_inf=[0.05, 0, 0], u_init=[0.05, 0, 0],
                        sponge=[0, 16, 8, 8, 8, 8], sponge_tau=1.0, sponge_sigma=0.1, total_pressure_inlet=True, storage=storage)
-        for l in range(1, 3):
+        for l in range(1, nl):
             d = s.dims(l - 1)
             n = [int(d[k] * 0.63) for k in range(3)]
             s.boxes.append(LevelBox(lo=[(d[k] - n[k]) // 2 for k in range(3)], n=n))
@@ -323,8 +348,11 @@ def d3q27_levels():
         ms = e0.elapsed_time(e1)
         cells = g.level_cells()
         lups = sum(c * 2 ** l for l, c in enumerate(cells)) / 2 ** (len(cells) - 1) * 64
-        res[storage.name.lower()] = round(lups / ms / 1e3, 1)
-        res["cells"] = cells
+        if nl == 1:
+            res["single_level_fp16"] = round(lups / ms / 1e3, 1)
+        else:
+            res[storage.name.lower()] = round(lups / ms / 1e3, 1)
+            res["cells"] = cells
         g.close()
     return res
 
@@ -483,6 +511,31 @@ def spin_overhead(steps: int = 100, warmup: int = 10):
     return out
 
 
+def voxelizer_times():
+    """The static voxelizer on the host cores (voxel.cpp, OpenMP) and on the
+    GPU (lbm_voxelize_static_gpu) for a sphere of radius 100 cells (81,920
+    triangles) in a 222^3 lattice, D3Q19 and D3Q27 links: seconds per call
+    (the GPU's after one warm-up call) and whether the results are identical."""
+    from simlab_b200.lbm import voxelize_static
+    from simlab_b200.shapes import sphere
+
+    v, t = sphere([110.3, 110.7, 110.1], 100.0, 6)
+    out = {"triangles": int(len(t)), "lattice_dims": [222, 222, 222]}
+    for lat in (19, 27):
+        t0 = time.perf_counter()
+        a = voxelize_static(v, t, [222] * 3, lat)
+        t_cpu = time.perf_counter() - t0
+        voxelize_static(v, t, [222] * 3, lat, device=True)
+        t0 = time.perf_counter()
+        b = voxelize_static(v, t, [222] * 3, lat, device=True)
+        t_gpu = time.perf_counter() - t0
+        same = bool(np.array_equal(a.solid, b.solid) and np.array_equal(a.walls.view(np.uint32), b.walls.view(np.uint32)))
+        out[f"d3q{lat}"] = {"cpu_s": round(t_cpu, 4), "gpu_s": round(t_gpu, 4), "walls": int(len(b.walls)), "solid": int(len(b.solid)),
+                            "identical": same}
+    out["cpu_threads"] = os.cpu_count()
+    return out
+
+
 def run_reference(args, ws, rank):
     """The reference arm: the oracle on the host cores, rank 0 only, on the
     same workload, metric and config as the engine's line; each step one
@@ -582,10 +635,16 @@ def main():
     if ws == 1 and not args.no_extras:
         line["adjoint"] = adjoint_ratio()
         line["d3q27_three_levels_mlups"] = d3q27_levels()
+        # the collision kernels' own update rates: the D3Q19 bulk kernel's
+        # event-timed duration, the single-level D3Q27 lattice's step
+        line["alu"] = alu_line({"d3q19_bulk_fp16": cells / (bulk_ms * 1e-3),
+                                "d3q27_step_fp16": line["d3q27_three_levels_mlups"]["single_level_fp16"] * 1e6},
+                               float((clocks or {}).get("sm_mhz") or 1965.0))
         line["c5_fp16_1024x512x512"] = c5_throughput()
         line["c5_adjoint"] = c5_adjoint()
         line["c3_rotor"] = c3_rotor()
         line["spin_overhead"] = spin_overhead()
+        line["voxelizer"] = voxelizer_times()
     if rank == 0 and ws == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_oracle_sample(budget_s=12.0)[0]
     if rank == 0:

@@ -267,6 +267,14 @@ int lbm_load_state(lbm_lattice *h, const void *buf, uint64_t bytes);
  * lbm_voxels_counts / lbm_voxels_copy and freed with lbm_voxels_free. */
 int lbm_voxelize_static(const double *verts, uint64_t nverts, const uint32_t *tris, uint64_t ntris,
                         const uint32_t dims[3], int32_t lattice, lbm_voxels **out);
+/* lbm_voxelize_static on the current CUDA device (no counterpart in the
+ * reference, which voxelizes on the CPU): the same solid cells and wall links,
+ * bit for bit (FP64 throughout, every product and sum rounded separately),
+ * returned in the same host handle.  Runs on a stream of its own and returns
+ * when the result is on the host; device scratch is allocated and freed
+ * within the call. */
+int lbm_voxelize_static_gpu(const double *verts, uint64_t nverts, const uint32_t *tris, uint64_t ntris,
+                            const uint32_t dims[3], int32_t lattice, lbm_voxels **out);
 int lbm_voxels_counts(const lbm_voxels *v, uint64_t *nsolid, uint64_t *nwalls);
 int lbm_voxels_copy(const lbm_voxels *v, uint32_t *solid, lbm_wall_cell *walls);
 void lbm_voxels_free(lbm_voxels *v);

@@ -17,7 +17,10 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 LIB = PKG / "libsimlab_lbm.so"
 
-CUDA_SOURCES = ["d3q19_kernels.cu", "lattice.cu", "noalloc.cu", "d3q27_kernels.cu", "mlattice.cu", "gray.cu"]
+CUDA_SOURCES = ["d3q19_kernels.cu", "lattice.cu", "noalloc.cu", "d3q27_kernels.cu", "mlattice.cu", "gray.cu", "voxel_gpu.cu"]
+# the GPU voxelizer rounds every product and sum separately, as the host
+# voxelizer does, so its results are bit-identical
+FILE_FLAGS = {"voxel_gpu.cu": ["-fmad=false"]}
 CXX_SOURCES = ["voxel.cpp"]
 HEADERS = ["lbm_device.cuh", "lbm_kernels.h", "voxel.hpp", "d3q27.h", "revoxel.cuh", "spin_math.cuh", "tma.cuh", "reduce.cuh"]
 
@@ -62,7 +65,7 @@ def build_library(force: bool = False, verbose: bool = False) -> Path:
     cmds = []
     for src in CUDA_SOURCES:
         obj = objdir / (src + ".o")
-        cmds.append(([cc, *ARCH, *NVCC_FLAGS, "-I", str(ROOT / "include"), "-c", str(CSRC / src), "-o", str(obj)], obj))
+        cmds.append(([cc, *ARCH, *NVCC_FLAGS, *FILE_FLAGS.get(src, []), "-I", str(ROOT / "include"), "-c", str(CSRC / src), "-o", str(obj)], obj))
     for src in CXX_SOURCES:
         obj = objdir / (src + ".o")
         cmds.append((["g++", "-O3", "-std=c++17", "-fPIC", "-fopenmp", "-c", str(CSRC / src), "-o", str(obj)], obj))

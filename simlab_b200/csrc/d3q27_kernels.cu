@@ -776,7 +776,8 @@ __device__ __forceinline__ bool in_box(const LevelParams &p, int lx, int ly, int
 
 __global__ void __launch_bounds__(BLK) k27_tri_scatter(const __grid_constant__ LevelParams p, const StepArgs a) {
     using namespace lbm::rv;
-    const uint32_t t = blockIdx.x * BLK + threadIdx.x;
+    // one warp per triangle, its lanes over the lattice points near it
+    const uint32_t t = (blockIdx.x * BLK + threadIdx.x) >> 5, lane = threadIdx.x & 31u;
     if (t >= p.ntri) return;
     const float4 t0 = p.tris[3 * t], t1 = p.tris[3 * t + 1], t2 = p.tris[3 * t + 2];
     const V3 ctr = {p.kf.center[0], p.kf.center[1], p.kf.center[2]};
@@ -796,9 +797,10 @@ __global__ void __launch_bounds__(BLK) k27_tri_scatter(const __grid_constant__ L
         lo[c] = max((int)ceilf(fs(mn[c], REACH)), p.box_lo[c]);
         hi[c] = min((int)floorf(fa(mx[c], REACH)), p.box_lo[c] + (int)p.box_n[c] - 1);
     }
-    for (int z = lo[2]; z <= hi[2]; z++)
-        for (int y = lo[1]; y <= hi[1]; y++)
-            for (int x = lo[0]; x <= hi[0]; x++) {
+    const int nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1, nz = hi[2] - lo[2] + 1;
+    const int npts = (nx > 0 && ny > 0 && nz > 0) ? nx * ny * nz : 0;
+    for (int q = (int)lane; q < npts; q += 32) {
+                const int x = lo[0] + q % nx, y = lo[1] + (q / nx) % ny, z = lo[2] + q / (nx * ny);
                 const V3 pt = {(float)x, (float)y, (float)z};
                 const float d0 = dot(nn, sub(pt, va));
                 if (fabsf(d0) > REACH) continue;
@@ -1098,7 +1100,7 @@ uint32_t reduce27_blocks(uint32_t nrec) { return (nrec + RED_BLK - 1) / RED_BLK;
 
 cudaError_t launch27_revoxel(int storage, const LevelParams &p, const StepArgs &a, cudaStream_t st) {
     if (!p.moving) return cudaSuccess;
-    if (p.ntri) k27_tri_scatter<<<blocks_for(p.ntri), BLK, 0, st>>>(p, a);
+    if (p.ntri) k27_tri_scatter<<<blocks_for((uint64_t)p.ntri * 32u), BLK, 0, st>>>(p, a);
     cudaError_t e = dispatch(storage, [&](auto *t) {
         using S = std::remove_pointer_t<decltype(t)>;
         k27_voxelize<S><<<blocks_for(p.nrec), BLK, 0, st>>>(p, a);

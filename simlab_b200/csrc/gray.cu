@@ -65,9 +65,12 @@ using lbm::WD;
 
 constexpr int BLK = 256;
 
+// feq_in: the inlet equilibrium (shifted by the weights); feq_q: the same
+// as the storage holds it (rounded to nearest in FP16 storage), which the
+// x = 1 cells pull from the inlet column
 template <class R>
 struct GConsts {
-    R omega, feq_in[19], center[3], dir[3];
+    R omega, feq_in[19], feq_q[19], center[3], dir[3];
 };
 
 struct GParams {
@@ -76,6 +79,10 @@ struct GParams {
     FastDiv div_nx, div_nxy;
     uint32_t box_lo[3], box_n[3];
     const void *a;       // R per cell: alpha * gamma (0 outside the design box)
+    // step-kernel blocks holding design-box cells: block b's slot among them
+    // (-1: none), so the force sum reads one partial per such block
+    const int32_t *box_slot;
+    uint32_t nbox_blocks;
     GConsts<float> kf;
     GConsts<double> kd;
 };
@@ -124,9 +131,10 @@ __device__ __forceinline__ double warp_sum(double v) {
     return v;
 }
 
-// per-block FP64 sums of 6 values; the last block to finish adds the block
-// partials in block order and writes out[0..5]
-__device__ __forceinline__ void block_reduce6(double *v, double *partials, uint32_t *ticket, double *out) {
+// Per-block FP64 sums of 6 values from the blocks that hold a slot (0 ..
+// count-1); the last of them to finish adds the partials in slot order and
+// writes out[0..5] (the order, so the sum, does not depend on scheduling)
+__device__ __forceinline__ void block_reduce6_at(double *v, uint32_t slot, uint32_t count, double *partials, uint32_t *ticket, double *out) {
     __shared__ double sh[BLK / 32][6];
     __shared__ bool last;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -138,16 +146,16 @@ __device__ __forceinline__ void block_reduce6(double *v, double *partials, uint3
     if (threadIdx.x < 6) {
         double t = 0;
         for (int w = 0; w < BLK / 32; w++) t += sh[w][threadIdx.x];
-        partials[blockIdx.x * 8 + threadIdx.x] = t;
+        partials[slot * 8 + threadIdx.x] = t;
         __threadfence();
     }
     __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == count - 1;
     __syncthreads();
     if (!last) return;
     __threadfence();
     double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (uint32_t b = threadIdx.x; b < gridDim.x; b += BLK)
+    for (uint32_t b = threadIdx.x; b < count; b += BLK)
         for (int j = 0; j < 6; j++) acc[j] += __ldcg(&partials[b * 8 + j]);
     for (int j = 0; j < 6; j++) acc[j] = warp_sum(acc[j]);
     __syncthreads();
@@ -184,41 +192,35 @@ __global__ void __launch_bounds__(BLK) kg_init(const __grid_constant__ GParams p
     for (int i = 0; i < 19; i++) P[(uint64_t)i * p.NP + n] = GS<S>::rn(k.feq_in[i]);
 }
 
-// x = 0: inlet equilibrium; x = NX-1: copy of x = NX-2
-template <class S>
-__global__ void __launch_bounds__(BLK) kg_faces(const __grid_constant__ GParams p, S *P) {
-    using R = typename GS<S>::R;
-    const uint32_t r = blockIdx.x * BLK + threadIdx.x;  // row (y, z)
-    if (r >= p.NY * p.NZ) return;
-    const GConsts<R> &k = KG<R>(p);
-    const uint32_t b0 = r * p.NX, b1 = b0 + p.NX - 1;
-#pragma unroll
-    for (int i = 0; i < 19; i++) {
-        P[(uint64_t)i * p.NP + b0] = GS<S>::rn(k.feq_in[i]);
-        P[(uint64_t)i * p.NP + b1] = P[(uint64_t)i * p.NP + b1 - 1];
-    }
-}
-
-// one step of the bulk (1 <= x <= NX-2).  MOM: (rho - 1, j) of every cell's
-// pre-collision state into 4 planes of NP; FORCE: a * j of every design-box
-// cell into 3 planes of the box (summed by kg_force).  FP16 storage rounds
-// stochastically from a hash of the cell and the step (seed_mix), so a
-// segment recomputed from its checkpoint repeats the first pass bit for bit.
+// one step of the bulk (1 <= x <= NX-2).  The x faces are read in place of
+// being written: the inlet column x = 0 holds the inlet equilibrium, so the
+// x = 1 cells pull feq_q for the directions coming from it; the outlet
+// column x = NX-1 is a copy of x = NX-2, so the x = NX-2 cells pull those
+// directions from their own column.  The face columns in memory are never
+// read.  MOM: (rho - 1, j) of every cell's
+// pre-collision state into 4 planes of NP; FORCE: the force a * j and its
+// moment about the centre of every design-box cell into fm, summed in FP64
+// over the grid (fixed order: block partials, then the last block).  FP16
+// storage rounds stochastically from a hash of the cell and the step
+// (seed_mix), so a segment recomputed from its checkpoint repeats the first
+// pass bit for bit.
 template <class S, bool MOM, bool FORCE>
-__global__ void __launch_bounds__(BLK) kg_step(const __grid_constant__ GParams p, const S *__restrict__ src, S *__restrict__ dst,
-                                               typename GS<S>::R *__restrict__ mom, typename GS<S>::R *__restrict__ fbox,
-                                               uint32_t seed_mix) {
+__device__ __forceinline__ void step_cell(const GParams &p, const S *__restrict__ src, S *__restrict__ dst, typename GS<S>::R *__restrict__ mom,
+                                          uint32_t seed_mix, uint32_t n, double *fm) {
     using R = typename GS<S>::R;
-    const uint32_t n = blockIdx.x * BLK + threadIdx.x;
-    if (n >= p.N) return;
     uint32_t x, y, z;
     coords(p, n, x, y, z);
     if (x < 1 || x + 1 >= p.NX) return;
     const GConsts<R> &k = KG<R>(p);
     const Off o = make_off(p, y, z);
     R g[19];
+    const bool outlet = x + 2 == p.NX;
 #pragma unroll
-    for (int i = 0; i < 19; i++) g[i] = lbm::Pop<S>::cvt(src[(uint64_t)i * p.NP + (uint32_t)((int32_t)n + o.at(-CX(i), -CY(i), -CZ(i)))]);
+    for (int i = 0; i < 19; i++) {
+        const int32_t dx = CX(i) == -1 ? (outlet ? 0 : 1) : -CX(i);
+        const R v = lbm::Pop<S>::cvt(src[(uint64_t)i * p.NP + (uint32_t)((int32_t)n + dx + o.at(0, -CY(i), -CZ(i)))]);
+        g[i] = (CX(i) == 1 && x == 1) ? k.feq_q[i] : v;
+    }
     R rho1 = 0, j[3] = {0, 0, 0};
 #pragma unroll
     for (int i = 0; i < 19; i++) {
@@ -248,36 +250,27 @@ __global__ void __launch_bounds__(BLK) kg_step(const __grid_constant__ GParams p
     if (FORCE) {
         const uint32_t bx = x - p.box_lo[0], by = y - p.box_lo[1], bz = z - p.box_lo[2];
         if (bx < p.box_n[0] && by < p.box_n[1] && bz < p.box_n[2]) {
-            const uint64_t nb = (uint64_t)p.box_n[0] * p.box_n[1] * p.box_n[2];
-            const uint64_t b = ((uint64_t)bz * p.box_n[1] + by) * p.box_n[0] + bx;
-            fbox[b] = an * j[0];
-            fbox[nb + b] = an * j[1];
-            fbox[2 * nb + b] = an * j[2];
+            const double F[3] = {(double)(an * j[0]), (double)(an * j[1]), (double)(an * j[2])};
+            const double r[3] = {(double)x - (double)k.center[0], (double)y - (double)k.center[1], (double)z - (double)k.center[2]};
+            fm[0] = F[0]; fm[1] = F[1]; fm[2] = F[2];
+            fm[3] = r[1] * F[2] - r[2] * F[1];
+            fm[4] = r[2] * F[0] - r[0] * F[2];
+            fm[5] = r[0] * F[1] - r[1] * F[0];
         }
     }
 }
 
-// force and moment about center on the gray body: FP64 sums over the box of
-// the per-cell a * j (fixed order: block partials, then the last block)
-template <class R>
-__global__ void __launch_bounds__(BLK) kg_force(const __grid_constant__ GParams p, const R *__restrict__ fbox, double *partials,
-                                                uint32_t *ticket, double *out) {
-    const uint64_t nb = (uint64_t)p.box_n[0] * p.box_n[1] * p.box_n[2];
-    const uint64_t b = (uint64_t)blockIdx.x * BLK + threadIdx.x;
+template <class S, bool MOM, bool FORCE>
+__global__ void __launch_bounds__(BLK, 4) kg_step(const __grid_constant__ GParams p, const S *__restrict__ src, S *__restrict__ dst,
+                                               typename GS<S>::R *__restrict__ mom, double *partials, uint32_t *ticket, double *out,
+                                               uint32_t seed_mix) {
+    const uint32_t n = blockIdx.x * BLK + threadIdx.x;
     double fm[6] = {0, 0, 0, 0, 0, 0};
-    if (b < nb) {
-        const GConsts<R> &k = KG<R>(p);
-        const uint32_t bx = (uint32_t)(b % p.box_n[0]), by = (uint32_t)((b / p.box_n[0]) % p.box_n[1]),
-                       bz = (uint32_t)(b / ((uint64_t)p.box_n[0] * p.box_n[1]));
-        const double F[3] = {(double)fbox[b], (double)fbox[nb + b], (double)fbox[2 * nb + b]};
-        const double r[3] = {(double)(p.box_lo[0] + bx) - (double)k.center[0], (double)(p.box_lo[1] + by) - (double)k.center[1],
-                             (double)(p.box_lo[2] + bz) - (double)k.center[2]};
-        fm[0] = F[0]; fm[1] = F[1]; fm[2] = F[2];
-        fm[3] = r[1] * F[2] - r[2] * F[1];
-        fm[4] = r[2] * F[0] - r[0] * F[2];
-        fm[5] = r[0] * F[1] - r[1] * F[0];
+    if (n < p.N) step_cell<S, MOM, FORCE>(p, src, dst, mom, seed_mix, n, fm);
+    if (FORCE) {
+        const int32_t slot = p.box_slot[blockIdx.x];  // the same for the whole block
+        if (slot >= 0) block_reduce6_at(fm, (uint32_t)slot, p.nbox_blocks, partials, ticket, out);
     }
-    block_reduce6(fm, partials, ticket, out);
 }
 
 // one reverse step t: lin = lambda of step t+1 (pre-collision adjoint),
@@ -367,7 +360,6 @@ struct lbm_gray {
     std::vector<void *> allocs;
     void *P[2] = {nullptr, nullptr};
     void *a = nullptr;
-    void *fbox = nullptr;  // a * j per design-box cell, 3 planes
     double *partials = nullptr;
     uint32_t *ticket = nullptr;
     double *hist = nullptr, *hist_host = nullptr;
@@ -386,7 +378,6 @@ struct lbm_gray {
 
     uint32_t nblk() const { return (p.N + gray::BLK - 1) / gray::BLK; }
     uint64_t nbox() const { return (uint64_t)p.box_n[0] * p.box_n[1] * p.box_n[2]; }
-    uint32_t box_blocks() const { return (uint32_t)((nbox() + gray::BLK - 1) / gray::BLK); }
     size_t set_bytes() const { return (size_t)19 * p.NP * ssz; }   // a population set (or checkpoint)
     size_t lset_bytes() const { return (size_t)19 * p.NP * rsz; }  // an adjoint set
     void *dalloc(size_t bytes) {
@@ -438,7 +429,7 @@ struct lbm_gray {
         cur = 0;
         steps_done = 0;
     }
-    // one forward step: faces on the current set, bulk into the other; out:
+    // one forward step, the current set into the other (faces read in place); out:
     // null (no forces) or 8 doubles for the force and moment of the step
     // stochastic-rounding seed of step steps_done + 1 (the engine's rule)
     uint32_t seed_mix() const {
@@ -449,15 +440,13 @@ struct lbm_gray {
         typed([&](auto *t) {
             using S = std::remove_pointer_t<decltype(t)>;
             using R = typename gray::GS<S>::R;
-            const uint32_t rows = p.NY * p.NZ, mix = seed_mix();
-            gray::kg_faces<S><<<(rows + gray::BLK - 1) / gray::BLK, gray::BLK, 0, stream>>>(p, (S *)P[cur]);
+            const uint32_t mix = seed_mix();
             const S *src = (const S *)P[cur];
             S *dst = (S *)P[1 - cur];
-            if (mom_slot && out) gray::kg_step<S, true, true><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, (R *)mom_slot, (R *)fbox, mix);
-            else if (mom_slot) gray::kg_step<S, true, false><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, (R *)mom_slot, nullptr, mix);
-            else if (out) gray::kg_step<S, false, true><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, nullptr, (R *)fbox, mix);
-            else gray::kg_step<S, false, false><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, nullptr, nullptr, mix);
-            if (out) gray::kg_force<R><<<box_blocks(), gray::BLK, 0, stream>>>(p, (const R *)fbox, partials, ticket, out);
+            if (mom_slot && out) gray::kg_step<S, true, true><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, (R *)mom_slot, partials, ticket, out, mix);
+            else if (mom_slot) gray::kg_step<S, true, false><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, (R *)mom_slot, nullptr, nullptr, nullptr, mix);
+            else if (out) gray::kg_step<S, false, true><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, nullptr, partials, ticket, out, mix);
+            else gray::kg_step<S, false, false><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, nullptr, nullptr, nullptr, nullptr, mix);
         });
         ck(cudaGetLastError(), "step kernel");
         cur = 1 - cur;
@@ -621,6 +610,9 @@ void fill(gray::GConsts<R> &k, const lbm_gray_setup &s) {
     for (int i = 0; i < 19; i++) {
         const double cu = lbm::CX(i) * s.u_in[0] + lbm::CY(i) * s.u_in[1] + lbm::CZ(i) * s.u_in[2];
         k.feq_in[i] = (R)(lbm::WD(i) * (3.0 * cu + 4.5 * cu * cu - usq));
+        k.feq_q[i] = k.feq_in[i];
+        if (s.storage == LBM_STORAGE_FP16)
+            k.feq_q[i] = (R)(__half2float(__float2half_rn((float)k.feq_in[i] * 32768.0f)) * (1.0f / 32768.0f));
     }
     for (int c = 0; c < 3; c++) { k.center[c] = (R)s.center[c]; k.dir[c] = (R)0; }
 }
@@ -656,8 +648,22 @@ void create_gray(const lbm_gray_setup *s, lbm_gray *h) {
     h->a = h->dalloc(N * h->rsz);
     ck(cudaMemsetAsync(h->a, 0, N * h->rsz, h->stream), "field init");
     p.a = h->a;
-    h->fbox = h->dalloc(3 * h->nbox() * h->rsz);
-    h->partials = (double *)h->dalloc((size_t)h->box_blocks() * 8 * 8);
+    {
+        // the step kernel's blocks that hold design-box cells, numbered in block order
+        std::vector<int32_t> slot(h->nblk(), -1);
+        for (uint32_t z = s->box_lo[2]; z < s->box_lo[2] + s->box_n[2]; z++)
+            for (uint32_t y = s->box_lo[1]; y < s->box_lo[1] + s->box_n[1]; y++)
+                for (uint32_t x = s->box_lo[0]; x < s->box_lo[0] + s->box_n[0]; x++)
+                    slot[(((uint64_t)z * s->dims[1] + y) * s->dims[0] + x) / gray::BLK] = 0;
+        uint32_t nb = 0;
+        for (auto &v : slot)
+            if (v == 0) v = (int32_t)nb++;
+        h->p.nbox_blocks = nb;
+        int32_t *d = (int32_t *)h->dalloc(slot.size() * 4);
+        ck(cudaMemcpy(d, slot.data(), slot.size() * 4, cudaMemcpyHostToDevice), "upload box blocks");
+        h->p.box_slot = d;
+        h->partials = (double *)h->dalloc((size_t)std::max<uint32_t>(nb, 1) * 8 * 8);
+    }
     h->ticket = (uint32_t *)h->dalloc(16);
     ck(cudaMemsetAsync(h->ticket, 0, 16, h->stream), "ticket init");
     h->hist = (double *)h->dalloc(HCHUNK * 8 * 8);

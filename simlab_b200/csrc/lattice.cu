@@ -952,6 +952,28 @@ int lbm_voxelize_static(const double *verts, uint64_t nverts, const uint32_t *tr
     });
 }
 
+int lbm_voxelize_static_gpu(const double *verts, uint64_t nverts, const uint32_t *tris, uint64_t ntris, const uint32_t dims[3],
+                            int32_t lattice, lbm_voxels **out) {
+    if (!out || !dims || (nverts && !verts) || (ntris && !tris)) { g_error = "null argument"; return LBM_ERR_INVALID; }
+    *out = nullptr;
+    return guard(nullptr, [&] {
+        if (lattice != 19 && lattice != 27) throw LbmError(LBM_ERR_INVALID, "lattice must be 19 or 27");
+        if (nverts >= 0xffffffffull || ntris >= 0xffffffffull) throw LbmError(LBM_ERR_INVALID, "surface too large");
+        lbm::Surface s = make_surface(verts, nverts, tris, ntris);
+        lbm_voxels *v = new lbm_voxels();
+        try {
+            v->v = lbm::voxelize_static_gpu(s, {dims[0], dims[1], dims[2]}, lattice);
+        } catch (const lbm::VoxelError &e) {
+            delete v;
+            throw LbmError(e.code == 2 ? LBM_ERR_NOMEM : (e.code == 3 ? LBM_ERR_CUDA : LBM_ERR_INVALID), e.what());
+        } catch (...) {
+            delete v;
+            throw;
+        }
+        *out = v;
+    });
+}
+
 int lbm_voxels_counts(const lbm_voxels *v, uint64_t *nsolid, uint64_t *nwalls) {
     if (!v) return LBM_ERR_INVALID;
     if (nsolid) *nsolid = v->v.solid.size();

@@ -34,7 +34,8 @@ __device__ __forceinline__ bool solid_at(const LatParams &p, const StepParams &s
 // shader.rs:902-940: one thread per triangle
 __global__ void __launch_bounds__(BLOCK) k_tri_scatter(const __grid_constant__ LatParams p, const __grid_constant__ StepParams s) {
     using namespace rv;
-    const uint32_t t = blockIdx.x * BLOCK + threadIdx.x;
+    // one warp per triangle, its lanes over the lattice points near it
+    const uint32_t t = (blockIdx.x * BLOCK + threadIdx.x) >> 5, lane = threadIdx.x & 31u;
     if (t >= p.ntri) return;
     const float4 t0 = p.tris[3 * t], t1 = p.tris[3 * t + 1], t2 = p.tris[3 * t + 2];
     const V3 ctr = {p.kf.center[0], p.kf.center[1], p.kf.center[2]};
@@ -52,9 +53,10 @@ __global__ void __launch_bounds__(BLOCK) k_tri_scatter(const __grid_constant__ L
     const int hi[3] = {min((int)floorf(fa(fmaxf(fmaxf(a.x, b.x), c.x), 1.415f)), p.box_lo[0] + (int)p.box_n[0] - 1),
                        min((int)floorf(fa(fmaxf(fmaxf(a.y, b.y), c.y), 1.415f)), p.box_lo[1] + (int)p.box_n[1] - 1),
                        min((int)floorf(fa(fmaxf(fmaxf(a.z, b.z), c.z), 1.415f)), p.box_lo[2] + (int)p.box_n[2] - 1)};
-    for (int z = lo[2]; z <= hi[2]; z++)
-        for (int y = lo[1]; y <= hi[1]; y++)
-            for (int x = lo[0]; x <= hi[0]; x++) {
+    const int nx = hi[0] - lo[0] + 1, ny = hi[1] - lo[1] + 1, nz = hi[2] - lo[2] + 1;
+    const int npts = (nx > 0 && ny > 0 && nz > 0) ? nx * ny * nz : 0;
+    for (int q = (int)lane; q < npts; q += 32) {
+                const int x = lo[0] + q % nx, y = lo[1] + (q / nx) % ny, z = lo[2] + q / (nx * ny);
                 const V3 pt = {(float)x, (float)y, (float)z};
                 const float d0 = dot(nn, sub(pt, a));
                 if (fabsf(d0) > 1.415f) continue;

@@ -3,6 +3,8 @@
 #include <array>
 #include <cstddef>
 #include <cstdint>
+#include <stdexcept>
+#include <string>
 #include <vector>
 
 namespace lbm {
@@ -45,5 +47,16 @@ Surface subdivide(const Surface &s, double max_edge);
 SpinVoxels voxelize_spin(const Surface &s, std::array<double, 3> axis, double h);
 bool seg_tri(const double o[3], const double d[3], const double t0[3], const double t1[3], const double t2[3], double *t);
 StaticVoxels voxelize_static(const Surface &s, std::array<size_t, 3> dims, int lattice);
+const std::vector<std::array<int, 3>> &dirs19();
+const std::vector<std::array<int, 3>> &dirs27();
+
+// Failure of the GPU voxelizer: code 1 internal, 2 out of device memory, 3 CUDA error
+struct VoxelError : std::runtime_error {
+    int code;
+    VoxelError(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+// voxelize_static on the current CUDA device: the same solid cells and wall
+// links, bit for bit
+StaticVoxels voxelize_static_gpu(const Surface &s, std::array<size_t, 3> dims, int lattice);
 
 }  // namespace lbm

@@ -194,6 +194,7 @@ def library() -> C.CDLL:
     L.lbm_save_state.argtypes = [vp, vp, u64]
     L.lbm_load_state.argtypes = [vp, vp, u64]
     L.lbm_voxelize_static.argtypes = [dp, u64, C.POINTER(C.c_uint32), u64, C.POINTER(C.c_uint32), i32, C.POINTER(vp)]
+    L.lbm_voxelize_static_gpu.argtypes = [dp, u64, C.POINTER(C.c_uint32), u64, C.POINTER(C.c_uint32), i32, C.POINTER(vp)]
     L.lbm_voxels_counts.argtypes = [vp, C.POINTER(u64), C.POINTER(u64)]
     L.lbm_voxels_copy.argtypes = [vp, C.POINTER(C.c_uint32), vp]
     L.lbm_voxels_free.argtypes = [vp]
@@ -589,14 +590,16 @@ def _surface_arrays(verts, tris):
     return v, t
 
 
-def voxelize_static(verts, tris, dims: Sequence[int], lattice: int = 19) -> StaticVoxels:
-    """voxelize_static / voxelize_static27 (voxel.rs:346-359)."""
+def voxelize_static(verts, tris, dims: Sequence[int], lattice: int = 19, device: bool = False) -> StaticVoxels:
+    """voxelize_static / voxelize_static27 (voxel.rs:346-359): on the host
+    cores, or with device=True on the current CUDA device
+    (lbm_voxelize_static_gpu, the same result bit for bit)."""
     L = library()
     v, t = _surface_arrays(verts, tris)
     d = (C.c_uint32 * 3)(*[int(x) for x in dims])
     h = C.c_void_p()
-    rc = L.lbm_voxelize_static(v.ctypes.data_as(C.POINTER(C.c_double)), len(v), t.ctypes.data_as(C.POINTER(C.c_uint32)), len(t), d,
-                               int(lattice), C.byref(h))
+    fn = L.lbm_voxelize_static_gpu if device else L.lbm_voxelize_static
+    rc = fn(v.ctypes.data_as(C.POINTER(C.c_double)), len(v), t.ctypes.data_as(C.POINTER(C.c_uint32)), len(t), d, int(lattice), C.byref(h))
     if rc != 0:
         raise _global_error(rc)
     try:

@@ -108,6 +108,7 @@ class SolverOptions:
     total_pressure_inlet: bool = True
     wall_model: bool = False
     refine: bool = True
+    gpu_voxelizer: bool = True             # static parts: voxelize on the device (the host voxelizer's result, bit for bit)
 
 
 def cells_across(q) -> int:
@@ -621,11 +622,11 @@ def run_with(cfg: WindConfig, m: Mesh, unit_m: float, opt: Optional[SolverOption
     elif p.multi is not None:
         b = p.multi.boxes[-1]
         fd = [2 * (b[1][k] - 1) + 1 for k in range(3)]
-        vox = voxelize_static(to_lat(m.positions) - np.asarray(p.multi.org_f), m.triangles, fd, lattice=27)
+        vox = voxelize_static(to_lat(m.positions) - np.asarray(p.multi.org_f), m.triangles, fd, lattice=27, device=opt.gpu_voxelizer)
         _thin_check(warnings, float(len(vox.solid)), m, p.dx)
         geom = vox
     else:
-        vox = voxelize_static(to_lat(m.positions), m.triangles, p.dims)
+        vox = voxelize_static(to_lat(m.positions), m.triangles, p.dims, device=opt.gpu_voxelizer)
         _thin_check(warnings, float(len(vox.solid)), m, p.dx)
         geom = vox
 

@@ -171,7 +171,7 @@ def test_run_loop_si_conversion_and_folder(monkeypatch, tmp_path):
     monkeypatch.setattr(lbm, "Lattice", _FakeLattice)
     _FakeLattice.made.clear()
     cfg, m = sphere_case(100.0, 16, duration=15.0)
-    r = T.run_with(cfg, m, 1e-3, T.SolverOptions())
+    r = T.run_with(cfg, m, 1e-3, T.SolverOptions(gpu_voxelizer=False))
     lat = _FakeLattice.made[-1]
     p = T.plan(cfg, m, 1e-3, T.SolverOptions())
     s = r.summary
@@ -212,7 +212,7 @@ def test_run_loop_spin_schedule(monkeypatch):
     monkeypatch.setattr(lbm, "Lattice", _FakeLattice)
     _FakeLattice.made.clear()
     cfg, m = rotating_sphere_case(1.0, 12, 2.0)
-    r = T.run_with(cfg, m, 1e-3, T.SolverOptions())
+    r = T.run_with(cfg, m, 1e-3, T.SolverOptions(gpu_voxelizer=False))
     lat = _FakeLattice.made[-1]
     p = T.plan(cfg, m, 1e-3, T.SolverOptions())
     a = np.concatenate(lat.calls)
