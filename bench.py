@@ -43,13 +43,13 @@ METRIC = "MLUPS (D3Q19 LES arm 512x256x256, FP16-stored populations)"
 UNIT = "MLUPS"
 DTYPE = "f32 arithmetic, fp16 storage"
 # Arithmetic per lattice update of the two collision kernels, FP16 storage,
-# from ncu's executed-instruction counts by opcode
-# (profiles/opcode_mix_k_bulk_tma_k27_step_fp16.md): flops = FADD + FMUL +
-# 2 FFMA per cell; instructions = all thread instructions per cell (D3Q19
-# includes the copy pipeline's wait loops).  FP32 peak: 148 SMs x 128 FP32
+# from ncu's counters (profiles/opcode_mix_k_bulk_tma_k27_step_fp16.md):
+# flops = FADD + FMUL + 2 FFMA thread instructions executed with the
+# predicate on, per cell; instructions = executed warp instructions x 32 per
+# cell (smsp__inst_executed; D3Q19 includes the copy pipeline's wait loops).  FP32 peak: 148 SMs x 128 FP32
 # lanes x 2 flops x clock; issue peak: 148 SMs x 4 schedulers x 32 threads x clock.
-ALU_PER_LUP = {"d3q19_bulk_fp16": {"flops": 85.7 + 50.6 + 2 * 71.4, "instr": 580.2},
-               "d3q27_step_fp16": {"flops": 161.5 + 175.0 + 2 * 177.0, "instr": 1012.0}}
+ALU_PER_LUP = {"d3q19_bulk_fp16": {"flops": 78.93 + 40.80 + 2 * 63.71, "instr": 410.8},
+               "d3q27_step_fp16": {"flops": 163.76 + 82.50 + 2 * 135.74, "instr": 1012.4}}
 
 
 def alu_line(lups: dict, sm_mhz: float) -> dict:

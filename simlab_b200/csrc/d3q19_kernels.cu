@@ -1213,34 +1213,23 @@ __global__ void __launch_bounds__(BLOCK) k_sample_slices(const __grid_constant__
 template <class S, int Q>
 __global__ void __launch_bounds__(BLOCK) k_mass(const __grid_constant__ LatParams p, double *scratch, double *out) {
     using R = typename Pop<S>::real;
-    constexpr int U = 4;  // cells per thread in flight: their loads go out together
     double v = 0, nbad = 0;
     const uint32_t stride = gridDim.x * BLOCK;
 #pragma unroll 1
-    for (uint64_t n0 = blockIdx.x * BLOCK + threadIdx.x; n0 < p.N; n0 += (uint64_t)U * stride) {
-        R f[U][19];
-        bool fluid[U];
+    for (uint32_t n = blockIdx.x * BLOCK + threadIdx.x; n < p.N; n += stride) {
+        const uint32_t fg = p.flags[n];
+        if ((fg & 3u) != 0u) continue;
+        uint32_t x, y, z;
+        coords(p, n, x, y, z);
+        const Nb nb = make_nb(p, x, y, z);
+        R f[19];
+        load_prev_out<S, Q>(p, n, nb, f);
+        double sum = 0;
 #pragma unroll
-        for (int u = 0; u < U; u++) {
-            const uint64_t n = n0 + (uint64_t)u * stride;
-            fluid[u] = n < p.N && (p.flags[n] & 3u) == 0u;
-            if (fluid[u]) {
-                uint32_t x, y, z;
-                coords(p, (uint32_t)n, x, y, z);
-                load_prev_out<S, Q>(p, (uint32_t)n, make_nb(p, x, y, z), f[u]);
-            }
-        }
-        // the cells in the order of a one-cell loop, so the sum is the same
-#pragma unroll
-        for (int u = 0; u < U; u++) {
-            if (!fluid[u]) continue;
-            double sum = 0;
-#pragma unroll
-            for (int i = 0; i < 19; i++) sum += (double)f[u][i];
-            const double rho = 1.0 + sum;
-            if (isfinite(rho)) v += rho;
-            else nbad += 1.0;
-        }
+        for (int i = 0; i < 19; i++) sum += (double)f[i];
+        const double rho = 1.0 + sum;
+        if (isfinite(rho)) v += rho;
+        else nbad += 1.0;
     }
     grid_sum2<BLOCK>(v, nbad, scratch, out);
 }
@@ -1366,7 +1355,7 @@ cudaError_t launch_dump(int storage, const LatParams &p, int q, cudaStream_t st)
     return cudaGetLastError();
 }
 
-uint32_t mass_blocks() { return (uint32_t)(2 * num_sms()); }
+uint32_t mass_blocks() { return (uint32_t)(4 * num_sms()); }
 
 template <class S>
 static void mass_s(const LatParams &p, int q, double *scratch, double *out, cudaStream_t st) {
