@@ -863,24 +863,48 @@ def run(cfg: WindConfig, m: Mesh, unit_m: float, progress=None) -> WindResult:
     return run_with(cfg, m, unit_m, SolverOptions(), progress)
 
 
+def _finite_range(a: np.ndarray) -> tuple[float, float]:
+    f = np.asarray(a, dtype=np.float32)
+    f = f[np.isfinite(f)]
+    return (0.0, 0.0) if f.size == 0 else (float(f.min()), float(f.max()))
+
+
 def write_run(r: WindResult, folder) -> None:
-    """A run folder (crates/cfd/examples/run_stl.rs:125-140): per-vertex
-    pressure and Cp as little-endian f32, each slice's header as JSON and
-    each of its fields as f32, the force history as CSV, and the summary as
-    run.json."""
+    """A wind run's folder as the engine stores it (docs/ARCHITECTURE.md
+    "Storage"; crates/engine/src/wind.rs:463-497): surface pressure and Cp
+    per mesh vertex as field.pressure.f32 / field.cp.f32 (little-endian f32),
+    each slice's header as slice.<name>.json and its fields as
+    slice.<name>.<field>.f32 (row-major in v then u), plus run.json (the
+    summary and the field and slice lists) and the force history as CSV."""
     d = Path(folder)
     d.mkdir(parents=True, exist_ok=True)
-    np.asarray(r.surface_pressure_pa, dtype="<f4").tofile(d / "pressure_pa.f32")
-    np.asarray(r.surface_cp, dtype="<f4").tofile(d / "cp.f32")
+    fields = []
+    if np.isfinite(r.surface_pressure_pa).any():
+        lo, hi = _finite_range(r.surface_pressure_pa)
+        np.asarray(r.surface_pressure_pa, dtype="<f4").tofile(d / "field.pressure.f32")
+        m = max(abs(lo), abs(hi))  # symmetric about zero: white is ambient
+        fields.append({"name": "pressure", "label": "Air pressure", "unit": "Pa", "min": -m, "max": m, "data_min": lo, "data_max": hi,
+                       "scale": "linear", "diverging": True})
+    if np.isfinite(r.surface_cp).any():
+        lo, hi = _finite_range(r.surface_cp)
+        np.asarray(r.surface_cp, dtype="<f4").tofile(d / "field.cp.f32")
+        fields.append({"name": "cp", "label": "Pressure coefficient", "unit": "", "min": lo, "max": hi, "scale": "linear", "diverging": True})
+    slices = []
     for s in r.slices:
+        if not s.fields:
+            continue
         hdr = {k: getattr(s, k) for k in ("name", "label", "origin_mm", "u_mm", "v_mm", "nu", "nv")}
-        hdr["fields"] = [{"name": f.name, "label": f.label, "unit": f.unit, "min": f.min if math.isfinite(f.min) else None,
-                          "max": f.max if math.isfinite(f.max) else None} for f in s.fields]
-        (d / f"slice.{s.name}.json").write_text(json.dumps(hdr, indent=2))
+        infos = []
         for f in s.fields:
+            lo, hi = _finite_range(f.data)
             np.asarray(f.data, dtype="<f4").tofile(d / f"slice.{s.name}.{f.name}.f32")
+            infos.append({"name": f.name, "label": f.label, "unit": f.unit, "min": lo, "max": hi})
+        hdr["fields"] = infos
+        (d / f"slice.{s.name}.json").write_text(json.dumps(hdr))
+        slices.append({"name": s.name, "label": s.label})
     with open(d / "history.csv", "w") as fh:
         fh.write("t,fx,fy,fz,mx,my,mz\n")
         for t, fv, mv in r.history:
             fh.write(",".join(repr(float(x)) for x in (t, *fv, *mv)) + "\n")
-    (d / "run.json").write_text(json.dumps(asdict(r.summary), indent=2))
+    run = {"kind": "wind", "summary": asdict(r.summary), "fields": fields, "slices": slices}
+    (d / "run.json").write_text(json.dumps(run, indent=2))

@@ -200,11 +200,16 @@ def test_run_loop_si_conversion_and_folder(monkeypatch, tmp_path):
     sp = r.slices[0].fields[0]
     assert sp.name == "speed" and sp.data[0] == pytest.approx(0.05 * p.dx / p.dt, rel=1e-6)
     T.write_run(r, tmp_path)
-    assert (tmp_path / "pressure_pa.f32").stat().st_size == 4 * len(m.positions)
+    # the engine's run folder (crates/engine/src/wind.rs:463-497)
+    assert (tmp_path / "field.pressure.f32").stat().st_size == 4 * len(m.positions)
+    assert np.array_equal(np.fromfile(tmp_path / "field.cp.f32", dtype="<f4"), r.surface_cp)
     hdr = json.loads((tmp_path / "slice.along.json").read_text())
     assert hdr["nu"] * hdr["nv"] * 4 == (tmp_path / "slice.along.speed.f32").stat().st_size
+    assert [f["name"] for f in hdr["fields"]] == ["speed", "pressure", "u", "v"]
     run = json.loads((tmp_path / "run.json").read_text())
-    assert run["kind"] == "wind" and run["converged"] and run["storage"] == "Fp32"
+    assert run["kind"] == "wind" and run["summary"]["converged"] and run["summary"]["storage"] == "Fp32"
+    assert [f["name"] for f in run["fields"]] == ["pressure", "cp"] and run["fields"][0]["min"] == -run["fields"][0]["max"]
+    assert [s["name"] for s in run["slices"]] == ["along", "across"]
     assert (tmp_path / "history.csv").read_text().splitlines()[0] == "t,fx,fy,fz,mx,my,mz"
 
 
