@@ -367,8 +367,12 @@ def c5_throughput(steps: int = 40, warmup: int = 4):
     from simlab_b200.cases import arm_les
     from simlab_b200.lbm import Lattice, Storage
 
+    t0 = time.perf_counter()
     st, vox = arm_les(Storage.FP16, scale=2)
+    t1 = time.perf_counter()
     lat = Lattice(st, vox)
+    lat.synchronize()
+    t2 = time.perf_counter()
     stream = torch.cuda.ExternalStream(lat.stream)
     lat.advance(warmup)
     lat.synchronize()
@@ -392,7 +396,8 @@ def c5_throughput(steps: int = 40, warmup: int = 4):
     hbm, _ = peaks()
     res = {"dims": list(st.dims), "cells": cells, "mlups": round(cells * steps / ms / 1e3, 1), "ms_per_step": round(ms / steps, 4),
            "bulk_ms": round(bulk_ms, 4), "bulk_hbm_frac": round(80.0 * cells / (bulk_ms * 1e-3) / 1e9 / hbm, 4),
-           "nonfinite": int(bad), "memory_gb": round(lat.info().memory_bytes / 1e9, 2)}
+           "nonfinite": int(bad), "memory_gb": round(lat.info().memory_bytes / 1e9, 2),
+           "setup_s": {"voxelize_host": round(t1 - t0, 3), "create": round(t2 - t1, 3)}}
     lat.close()
     return res
 

@@ -418,8 +418,17 @@ __global__ void __launch_bounds__(BLOCK) k_faces(const __grid_constant__ LatPara
         if (blockIdx.x < p.fblk[g + 1]) F = g;
     const uint32_t kf = p.fplan[F] + (blockIdx.x - p.fblk[F]) * BLOCK + threadIdx.x;
     if (kf >= (F < 6 ? p.fplan[F + 1] : s.nface)) return;
-    const uint32_t b = p.faces[kf];
-    const uint32_t info = p.face_info[kf];
+    uint32_t b, info;
+    if (F < 6 && p.frect[F]) {
+        // the face's rectangle in cell order: the cell from its rank, no list
+        // load before the neighbour's populations
+        const uint32_t k = kf - p.fplan[F], v = p.frect_nu[F].div(k), u = k - v * p.frect_nu[F].d;
+        b = p.frect_b0[F] + u + v * p.frect_sv[F];
+        info = p.finfo[F];
+    } else {
+        b = p.faces[kf];
+        info = p.face_info[kf];
+    }
     switch (F) {
         case 0: face_planar<S, Q, 0>(p, s, b, info); return;
         case 1: face_planar<S, Q, 1>(p, s, b, info); return;

@@ -398,6 +398,8 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
         }
     }
     uint32_t fplan[7] = {0, 0, 0, 0, 0, 0, 0}, fblk[7] = {0, 0, 0, 0, 0, 0, 0};
+    uint32_t rect[6] = {0, 0, 0, 0, 0, 0}, rect_b0[6] = {0, 0, 0, 0, 0, 0}, rect_sv[6] = {0, 0, 0, 0, 0, 0},
+             rect_nu[6] = {1, 1, 1, 1, 1, 1}, rect_info[6] = {0, 0, 0, 0, 0, 0};
     {
         // face cells are independent; grouping them by kind and store mask
         // keeps each warp on one code path.  Planar cells of a velocity or
@@ -427,6 +429,26 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
         for (int f = 1; f < 7; f++) {
             fplan[f] = fplan[f - 1] + cnt[f - 1];
             fblk[f] = fblk[f - 1] + (cnt[f - 1] + (uint32_t)lbm::BLOCK - 1) / (uint32_t)lbm::BLOCK;
+        }
+        // a y or z face's planar group is the rectangle x in [2, NX-3] by the
+        // other in-plane axis in [2, N-3] (interior points of non-periodic
+        // axes), listed in cell order; checked cell by cell before the face
+        // kernel relies on it
+        for (int f = 2; f < 6; f++) {
+            const int a = f >> 1, o = a == 1 ? 2 : 1;
+            const uint64_t nu = NX >= 5 ? NX - 4 : 0, nv = dimv[o] >= 5 ? dimv[o] - 4 : 0;
+            const uint64_t fixed = (f & 1) ? dimv[a] - 1 : 0;
+            const uint64_t so = o == 1 ? NX : NX * NY, sa = a == 1 ? NX : NX * NY;
+            const uint64_t b0 = 2 + 2 * so + fixed * sa;
+            bool ok = cnt[f] > 0 && (uint64_t)cnt[f] == nu * nv;
+            for (uint64_t k = 0; ok && k < cnt[f]; k++) ok = faces[ord[fplan[f] + k]] == b0 + k % nu + (k / nu) * so;
+            rect[f] = ok ? 1u : 0u;
+            if (ok) {
+                rect_b0[f] = (uint32_t)b0;
+                rect_sv[f] = (uint32_t)so;
+                rect_nu[f] = (uint32_t)nu;
+                rect_info[f] = finfo[ord[fplan[f]]];
+            }
         }
         std::vector<uint32_t> f2(faces.size()), i2(faces.size());
         uint32_t rest = 0;
@@ -542,6 +564,13 @@ void create_impl(const lbm_setup *setup, const lbm_geometry *geom, const lbm_pro
     p.xface_info[0] = xinfo[0];
     p.xface_info[1] = xinfo[1];
     for (int f = 0; f < 7; f++) { p.fplan[f] = fplan[f]; p.fblk[f] = fblk[f]; }
+    for (int f = 0; f < 6; f++) {
+        p.frect[f] = rect[f];
+        p.frect_b0[f] = rect_b0[f];
+        p.frect_sv[f] = rect_sv[f];
+        p.finfo[f] = rect_info[f];
+        p.frect_nu[f].init(rect_nu[f]);
+    }
     // sponge ramps per axis (shader.rs:528-538): 1 - p / width inside a layer
     std::vector<float> tabf;
     std::vector<double> tabd;

@@ -141,6 +141,12 @@ struct LatParams {
     // fplan[F]: first list index of group F (F = 6: the rest); fblk[F]: the
     // face kernel's first block for group F.
     uint32_t fplan[7], fblk[7];
+    // A planar group of a y or z face that lists its whole rectangle in cell
+    // order (frect[F] = 1): cell k of the group is frect_b0 + u + v frect_sv
+    // with k = v nu + u, nu = frect_nu.d, so the face kernel computes it and
+    // the group's info (finfo[F]) instead of loading them.
+    uint32_t frect[6], frect_b0[6], frect_sv[6], finfo[6];
+    FastDiv frect_nu[6];
     int tma;                   // the staged bulk kernel applies (NX * element size % 16 == 0)
     // spinning part (Geometry::Spin, lattice.rs:87-92): every cell of the swept
     // box is a record, re-voxelized each step from the rotated surface

@@ -388,21 +388,29 @@ def plan(cfg: WindConfig, m: Mesh, unit_m: float, opt: SolverOptions, budget: Op
         return n * (19 * _pop_bytes(s) + 4) + est_records * 40 * 4 + faces_cells * 44 + 64 * 1024 * 1024
 
     n_max = max(multi.cells) if multi is not None else n
-    fits_layout = n_max < (1 << 32) - 1  # 32-bit cell indices per level
+
+    def fits_layout(s: int) -> bool:
+        # this engine's limits: 32-bit cell indices per level (refined), the
+        # single lattice's own bound per storage (lbm_max_cells)
+        if multi is not None:
+            return n_max < (1 << 32) - 1
+        from .lbm import library
+        return n <= int(library().lbm_max_cells(int(s)))
+
     bud = budget if budget is not None else opt.memory_budget
     if opt.storage is not None:
         storage = int(opt.storage)
-    elif bud is not None and mem_for(int(Storage.FP32)) > bud:
+    elif (bud is not None and mem_for(int(Storage.FP32)) > bud) or not fits_layout(int(Storage.FP32)):
         storage = int(Storage.FP16)
     else:
         storage = int(Storage.FP32)
-    memory = mem_for(storage) if fits_layout else (1 << 62)
+    memory = mem_for(storage) if fits_layout(storage) else (1 << 62)
     frontal = math.pi * rotor_radius ** 2 if still else frontal_area(m, r)
     blockage = frontal / ((dom_hi[1] - dom_lo[1]) * (dom_hi[2] - dom_lo[2]))
     dxs = dx * ((dims[0] - 1) / (multi.dims0[0] - 1)) if multi is not None else dx  # sponge widths in coarsest cells
 
     def cl(x, lo_):
-        return int(max(round(x / dxs), lo_))
+        return int(max(_round_away(x / dxs), lo_))
 
     if still:
         sp = cl(opt.sponge_widths[2] * d_front, 8)
