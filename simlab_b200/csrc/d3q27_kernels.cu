@@ -316,7 +316,9 @@ template <bool WRAP> struct StepOcc<double, WRAP> { static constexpr int value =
 // One cell's update once its 27 pulled populations f (storage units) are
 // in registers: walls, cumulant collision, stores into the other set, the
 // moments the neighbouring levels read (mshader.rs:199-403,612-699).
-template <class S, bool FORCE>
+// SPONGE: the level has sponge layers (viscosity ramp and absorbing layer);
+// without them the code is left out, not predicated off per lane
+template <class S, bool FORCE, bool SPONGE>
 __device__ __forceinline__ void cell27(const LevelParams &p, const StepArgs &a, uint32_t n, uint32_t fg, uint32_t x, uint32_t y, uint32_t z,
                                        typename Pop<S>::real *f) {
     using R = typename Pop<S>::real;
@@ -408,7 +410,7 @@ __device__ __forceinline__ void cell27(const LevelParams &p, const StepArgs &a, 
         tau = (R)0.5 * (k.tau0 + sqrt(k.tau0 * k.tau0 + (R)18 * k.smag2 * sqrt((R)2 * pp) * inv_rho));
     }
     R sp = 0;
-    if (p.n_sponge) {
+    if (SPONGE && p.n_sponge) {
         sp = sponge<R>(p, k, x, y, z);
         if (sp > (R)0 && k.sponge_tau > tau) tau += sp * sp * (k.sponge_tau - tau);
     }
@@ -427,7 +429,7 @@ __device__ __forceinline__ void cell27(const LevelParams &p, const StepArgs &a, 
     }
     // absorbing layer (mshader.rs:663-673): fo += sigma sp^2 (feq(1, ut) - feq(rho, u)),
     // both product-form equilibria, so per direction a product of axis factors
-    const bool absorb = p.n_sponge && k.sigma > (R)0 && sp > (R)0;
+    const bool absorb = SPONGE && p.n_sponge && k.sigma > (R)0 && sp > (R)0;
     R at[3][3], ac[3][3], sgm = 0;
     if (absorb) {
         const R h = (R)0.5;
@@ -446,7 +448,7 @@ __device__ __forceinline__ void cell27(const LevelParams &p, const StepArgs &a, 
     R pend = 0;
     int pend_i = -1;
     gauss_raw<R, FORCE>(u, sg, m1, rs, SC, [&](int i, R v) {
-        if (absorb) {
+        if (SPONGE && absorb) {
             const int ix = CX(i) + 1, iy = CY(i) + 1, iz = CZ(i) + 1;
             v += sgm * (at[0][ix] * at[1][iy] * at[2][iz] - rho * ac[0][ix] * ac[1][iy] * ac[2][iz]);
         }
@@ -484,7 +486,7 @@ __device__ __forceinline__ void cell27(const LevelParams &p, const StepArgs &a, 
 }
 
 
-template <class S, bool FORCE, bool WRAP>
+template <class S, bool FORCE, bool WRAP, bool SPONGE>
 __global__ void __launch_bounds__(BLK, StepOcc<S, WRAP>::value) k27_step(const __grid_constant__ LevelParams p, const StepArgs a) {
     using R = typename Pop<S>::real;
     const uint32_t n = blockIdx.x * BLK + threadIdx.x;
@@ -510,7 +512,7 @@ __global__ void __launch_bounds__(BLK, StepOcc<S, WRAP>::value) k27_step(const _
 #pragma unroll
         for (int i = 0; i < 27; i++) f[i] = Raw<S>::ld(srcn + ((int64_t)i * NP - CX(i) * SX - CY(i) * SY - CZ(i) * SZ));
     }
-    cell27<S, FORCE>(p, a, n, fg, x, y, z, f);
+    cell27<S, FORCE, SPONGE>(p, a, n, fg, x, y, z, f);
 }
 
 // ------------------------------------------------------------ level kernels
@@ -1019,12 +1021,24 @@ cudaError_t launch27_step(int storage, const LevelParams &p, const StepArgs &a, 
     return dispatch(storage, [&](auto *t) {
         using S = std::remove_pointer_t<decltype(t)>;
         const bool wrap = p.per[0] || p.per[1] || p.per[2];
+        const unsigned g = blocks_for(p.N);
+        const bool sp = p.n_sponge != 0;
         if (p.forcing) {
-            if (wrap) k27_step<S, true, true><<<blocks_for(p.N), BLK, 0, st>>>(p, a);
-            else k27_step<S, true, false><<<blocks_for(p.N), BLK, 0, st>>>(p, a);
+            if (wrap) {
+                if (sp) k27_step<S, true, true, true><<<g, BLK, 0, st>>>(p, a);
+                else k27_step<S, true, true, false><<<g, BLK, 0, st>>>(p, a);
+            } else {
+                if (sp) k27_step<S, true, false, true><<<g, BLK, 0, st>>>(p, a);
+                else k27_step<S, true, false, false><<<g, BLK, 0, st>>>(p, a);
+            }
         } else {
-            if (wrap) k27_step<S, false, true><<<blocks_for(p.N), BLK, 0, st>>>(p, a);
-            else k27_step<S, false, false><<<blocks_for(p.N), BLK, 0, st>>>(p, a);
+            if (wrap) {
+                if (sp) k27_step<S, false, true, true><<<g, BLK, 0, st>>>(p, a);
+                else k27_step<S, false, true, false><<<g, BLK, 0, st>>>(p, a);
+            } else {
+                if (sp) k27_step<S, false, false, true><<<g, BLK, 0, st>>>(p, a);
+                else k27_step<S, false, false, false><<<g, BLK, 0, st>>>(p, a);
+            }
         }
         return cudaGetLastError();
     });
