@@ -219,6 +219,11 @@ typedef struct {
     double bulk_ms;
     uint64_t launches;
 } lbm_kernel_times;
+/* Per-kernel device timing of the following steps with CUDA events on the
+ * lattice's streams: enable 1 times the face, wall and bulk kernels (four
+ * events per step), 2 only the bulk kernel (two events per step, so the
+ * timed steps carry fewer stream operations; faces_ms and walls_ms stay 0),
+ * 0 stops.  Starting clears the totals. */
 int lbm_profile(lbm_lattice *h, int32_t enable);
 int lbm_get_kernel_times(lbm_lattice *h, lbm_kernel_times *out);
 

@@ -1282,7 +1282,7 @@ static void launch_tma(const LatParams &p, const StepParams &s, cudaStream_t st)
 template <class S, int P, int COLL>
 static cudaError_t step_t(const LatParams &p, const StepParams &s, cudaStream_t st, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join,
                           cudaEvent_t *ev) {
-    if (ev) cudaEventRecord(ev[0], st);
+    if (ev && ev[0]) cudaEventRecord(ev[0], st);
     if (p.moving) {
         // re-voxelize the spinning part's swept box for this step's rotation
         // (lattice.rs:719-723): triangles -> link scratch, cells, scratch reset
@@ -1298,10 +1298,10 @@ static cudaError_t step_t(const LatParams &p, const StepParams &s, cudaStream_t 
         cudaEventRecord(join, side);
     }
     if (s.nface) k_faces<S, P><<<p.fblk[6] + blocks_for(s.nface - p.fplan[6]), BLOCK, 0, st>>>(p, s);
-    if (ev) cudaEventRecord(ev[1], st);
+    if (ev && ev[1]) cudaEventRecord(ev[1], st);
     if (overlap) cudaStreamWaitEvent(st, join, 0);
     else if (p.nrec) k_walls<S, P, COLL><<<(unsigned)((p.nrec + WBLOCK - 1) / WBLOCK), WBLOCK, 0, st>>>(p, s);
-    if (ev) cudaEventRecord(ev[2], st);
+    if (ev && ev[2]) cudaEventRecord(ev[2], st);
     if (p.tma) {
         if (!p.forcing && !p.abs_u) {
             if (p.les_on) launch_tma<S, P, COLL, 3>(p, s, st);
@@ -1312,7 +1312,7 @@ static cudaError_t step_t(const LatParams &p, const StepParams &s, cudaStream_t 
     } else {
         k_bulk<S, P, COLL><<<blocks_for(p.N), BLOCK, 0, st>>>(p, s);
     }
-    if (ev) cudaEventRecord(ev[3], st);
+    if (ev && ev[3]) cudaEventRecord(ev[3], st);
     return cudaGetLastError();
 }
 

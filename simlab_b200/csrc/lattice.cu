@@ -91,8 +91,10 @@ struct lbm_lattice {
     float voff = 0.f;
     double *hist_host = nullptr;  // pinned
     cudaEvent_t ev = nullptr;
-    // kernel profiling: 4 events per profiled step
+    // kernel profiling: 4 events per profiled step (mode 1), or only the two
+    // around the bulk kernel (mode 2)
     bool prof = false;
+    int prof_mode = 0;
     std::vector<cudaEvent_t> prof_ev;
     uint64_t prof_steps = 0;
     uint64_t prof_launches = 0;  // kernels launched by the profiled steps
@@ -647,6 +649,7 @@ void run_impl(lbm_lattice *h, const lbm_step_in *steps, uint64_t n, double *forc
             const uint64_t idx = h->steps_done;
             lbm::StepParams sp = step_params(h, si, k, idx);
             cudaEvent_t *evs = nullptr;
+            cudaEvent_t ev4[4];
             if (h->prof) {
                 const size_t need = 4 * (h->prof_steps + 1);
                 while (h->prof_ev.size() < need) {
@@ -655,6 +658,11 @@ void run_impl(lbm_lattice *h, const lbm_step_in *steps, uint64_t n, double *forc
                     h->prof_ev.push_back(e);
                 }
                 evs = h->prof_ev.data() + 4 * h->prof_steps;
+                if (h->prof_mode == 2) {
+                    // bulk kernel only: the face and wall events are not recorded
+                    ev4[0] = nullptr; ev4[1] = nullptr; ev4[2] = evs[2]; ev4[3] = evs[3];
+                    evs = ev4;
+                }
                 h->prof_steps++;
                 // the kernels launch_step enqueues for this step
                 h->prof_launches += (sp.nface ? 1u : 0u) + (p.nrec ? 1u : 0u) + 1u + (p.moving ? 2u + (p.ntri ? 1u : 0u) : 0u);
@@ -751,7 +759,9 @@ int lbm_profile(lbm_lattice *h, int32_t enable) {
     if (!h) return LBM_ERR_INVALID;
     return guard(h, [&] {
         h->wait();
+        if (enable < 0 || enable > 2) throw LbmError(LBM_ERR_INVALID, "profile mode must be 0, 1 or 2");
         h->prof = enable != 0;
+        h->prof_mode = enable;
         h->prof_steps = 0;
         h->prof_launches = 0;
     });
@@ -766,9 +776,11 @@ int lbm_get_kernel_times(lbm_lattice *h, lbm_kernel_times *out) {
         out->faces_ms = out->walls_ms = out->bulk_ms = 0.0;
         for (uint64_t k = 0; k < h->prof_steps; k++) {
             cudaEvent_t *e = h->prof_ev.data() + 4 * k;
-            float a, b, c;
-            ck(cudaEventElapsedTime(&a, e[0], e[1]), "cudaEventElapsedTime");
-            ck(cudaEventElapsedTime(&b, e[1], e[2]), "cudaEventElapsedTime");
+            float a = 0, b = 0, c;
+            if (h->prof_mode != 2) {
+                ck(cudaEventElapsedTime(&a, e[0], e[1]), "cudaEventElapsedTime");
+                ck(cudaEventElapsedTime(&b, e[1], e[2]), "cudaEventElapsedTime");
+            }
             ck(cudaEventElapsedTime(&c, e[2], e[3]), "cudaEventElapsedTime");
             out->faces_ms += a;
             out->walls_ms += b;

@@ -512,9 +512,11 @@ class Lattice:
     def set_timeout(self, seconds: float) -> None:
         self._check(self._L.lbm_set_timeout(self._h, float(seconds)))
 
-    def profile(self, enable: bool) -> None:
-        """Starts (clearing the totals) or stops per-kernel event timing."""
-        self._check(self._L.lbm_profile(self._h, int(bool(enable))))
+    def profile(self, enable) -> None:
+        """Starts (clearing the totals) or stops per-kernel event timing:
+        True or 1 times faces, walls and bulk; 2 only the bulk kernel; False
+        or 0 stops."""
+        self._check(self._L.lbm_profile(self._h, int(enable)))
 
     def kernel_times(self) -> dict:
         """Device milliseconds per kernel summed over the profiled steps."""
