@@ -316,6 +316,14 @@ def adjoint_ratio():
         out["recompute_all" if rc else "memory_sized"] = {"backward_ms": round(tot, 3), "ratio": round(tot / fwd, 3),
                                                            **{k: round(v, 3) for k, v in t.items()}}
     out["adjoint_over_forward"] = out["recompute_all"]["ratio"]
+    # bytes per cell and step (FP32): forward 19 loads + 19 stores + a; the
+    # recomputing step also writes rho - 1 and j; the reverse step reads and
+    # writes lambda and reads the moments and a
+    cells = 192 * 96 * 96
+    hbm, _ = peaks()
+    out["bytes_per_cell"] = {"forward": 156, "recompute": 172, "reverse": 172}
+    out["hbm_frac"] = {"forward": round(156 * cells * spec.steps / (fwd * 1e-3) / 1e9 / hbm, 3),
+                       "reverse": round(172 * cells * spec.steps / (out["recompute_all"]["reverse_ms"] * 1e-3) / 1e9 / hbm, 3)}
     out["objective"] = J
     lat.close()
     return out
