@@ -307,8 +307,14 @@ __device__ __forceinline__ void gauss_raw(const R *u, const R *sg, const R *m1, 
 // Register budget (blocks of 256 threads per SM): FP32/FP16/BF16 without
 // periodic wrap run 3 (80 registers, a few spilled to L1), with wrap 2; the
 // FP64 engine (a validation instrument) keeps the compiler's choice.
-template <class S, bool WRAP> struct StepOcc { static constexpr int value = WRAP ? 2 : 3; };
-template <bool WRAP> struct StepOcc<double, WRAP> { static constexpr int value = 1; };
+// Blocks per SM the step kernel is compiled for.  Without periodic axes and
+// sponges, 2-byte storage runs four blocks (64 registers, a few words
+// spilled; measured +6 % on the three-level lattice); FP32, and the sponge
+// variants, lose more to the spills than they gain and run three.
+template <class S, bool WRAP, bool SPONGE> struct StepOcc {
+    static constexpr int value = WRAP ? 2 : ((sizeof(S) == 2 && !SPONGE) ? 4 : 3);
+};
+template <bool WRAP, bool SPONGE> struct StepOcc<double, WRAP, SPONGE> { static constexpr int value = 1; };
 
 // WRAP: the level has periodic axes (neighbour offsets per thread); without
 // them no stepped cell touches the boundary, and every neighbour offset is
@@ -487,7 +493,7 @@ __device__ __forceinline__ void cell27(const LevelParams &p, const StepArgs &a, 
 
 
 template <class S, bool FORCE, bool WRAP, bool SPONGE>
-__global__ void __launch_bounds__(BLK, StepOcc<S, WRAP>::value) k27_step(const __grid_constant__ LevelParams p, const StepArgs a) {
+__global__ void __launch_bounds__(BLK, StepOcc<S, WRAP, SPONGE>::value) k27_step(const __grid_constant__ LevelParams p, const StepArgs a) {
     using R = typename Pop<S>::real;
     const uint32_t n = blockIdx.x * BLK + threadIdx.x;
     if (n >= p.N) return;
