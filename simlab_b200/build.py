@@ -22,7 +22,7 @@ CUDA_SOURCES = ["d3q19_kernels.cu", "lattice.cu", "noalloc.cu", "d3q27_kernels.c
 # voxelizer does, so its results are bit-identical
 FILE_FLAGS = {"voxel_gpu.cu": ["-fmad=false"]}
 CXX_SOURCES = ["voxel.cpp"]
-HEADERS = ["lbm_device.cuh", "lbm_kernels.h", "voxel.hpp", "d3q27.h", "revoxel.cuh", "spin_math.cuh", "tma.cuh", "reduce.cuh"]
+HEADERS = ["lbm_device.cuh", "lbm_kernels.h", "voxel.hpp", "d3q27.h", "revoxel.cuh", "spin_math.cuh", "tma.cuh", "reduce.cuh", "host_wait.hpp"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-prec-div=false", "-prec-sqrt=false", "-Xcompiler", "-fPIC,-fopenmp",

@@ -50,6 +50,7 @@
 
 #include "../../include/simlab_lbm.h"
 #include "lbm_device.cuh"
+#include "host_wait.hpp"
 
 namespace lbm_host {
 void set_global_error(const std::string &msg);
@@ -394,7 +395,10 @@ struct lbm_gray {
         q = nullptr;
     }
     ~lbm_gray() {
-        if (stream) cudaStreamSynchronize(stream);
+        if (stream && lbm::stream_wait(stream, timeout_s) == cudaErrorTimeout) {
+            lbm_host::set_global_error("gray lattice destroyed while its device work had not finished: buffers left allocated");
+            return;
+        }
         for (void *q : allocs) cudaFree(q);
         if (hist_host) cudaFreeHost(hist_host);
         if (ev) cudaEventDestroy(ev);

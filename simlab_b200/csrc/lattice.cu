@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/simlab_lbm.h"
+#include "host_wait.hpp"
 #include "lbm_kernels.h"
 #include "voxel.hpp"
 
@@ -112,13 +113,18 @@ struct lbm_lattice {
         return p;
     }
     ~lbm_lattice() {
-        if (stream) cudaStreamSynchronize(stream);
+        // bounded waits: if the device never finishes, the buffers it may
+        // still use are left allocated rather than freed under it
+        if ((stream && lbm::stream_wait(stream, timeout_s) == cudaErrorTimeout) ||
+            (side && lbm::stream_wait(side, timeout_s) == cudaErrorTimeout)) {
+            lbm_host::set_global_error("lattice destroyed while its device work had not finished: buffers left allocated");
+            return;
+        }
         for (void *p : allocs) cudaFree(p);
         if (hist_host) cudaFreeHost(hist_host);
         if (err_host) cudaFreeHost(err_host);
         if (ev) cudaEventDestroy(ev);
         for (cudaEvent_t e : prof_ev) cudaEventDestroy(e);
-        if (side) cudaStreamSynchronize(side);
         if (fork) cudaEventDestroy(fork);
         if (join) cudaEventDestroy(join);
         if (side) cudaStreamDestroy(side);

@@ -22,6 +22,7 @@
 
 #include "../../include/simlab_lbm.h"
 #include "d3q27.h"
+#include "host_wait.hpp"
 
 namespace lbm_host {
 void set_global_error(const std::string &msg);
@@ -108,7 +109,10 @@ struct lbm_multi {
         return p;
     }
     ~lbm_multi() {
-        if (stream) cudaStreamSynchronize(stream);
+        if (stream && lbm::stream_wait(stream, timeout_s) == cudaErrorTimeout) {
+            lbm_host::set_global_error("multi-level lattice destroyed while its device work had not finished: buffers left allocated");
+            return;
+        }
         for (void *p : allocs) cudaFree(p);
         if (hist_host) cudaFreeHost(hist_host);
         if (ev) cudaEventDestroy(ev);
@@ -263,7 +267,7 @@ void init_moments(lbm_multi *h, void *dst, uint64_t nodes, const lbm_multi_setup
         c[10] = (R)tau_l;
     }
     ck(cudaMemcpyAsync(dst, v.data(), v.size() * sizeof(R), cudaMemcpyHostToDevice, h->stream), "moment init");
-    ck(cudaStreamSynchronize(h->stream), "moment init");
+    ck(lbm::stream_wait(h->stream, h->timeout_s), "moment init");
 }
 
 void create_multi(const lbm_multi_setup *setup, const lbm_geometry *geom, const lbm_probes *probes, lbm_multi *h) {
@@ -508,7 +512,7 @@ void create_multi(const lbm_multi_setup *setup, const lbm_geometry *geom, const 
         p.faces = upload_list(faces);
         p.ghosts = upload_list(ghosts);
         p.restricted = upload_list(restricted);
-        ck(cudaStreamSynchronize(h->stream), "upload");
+        ck(lbm::stream_wait(h->stream, h->timeout_s), "upload");
         const double tau_l = 0.5 + 3.0 * s.nu0 * (double)(1ull << l);
         if (p.has_child) {
             p.mom_child = h->dalloc(2ull * p.ch_nodes * lbm27::MW * rsz);
@@ -550,7 +554,7 @@ void create_multi(const lbm_multi_setup *setup, const lbm_geometry *geom, const 
         if (!pix_lists[l].empty())
             ck(cudaMemcpyAsync(h->pix[l], pix_lists[l].data(), pix_lists[l].size() * 4, cudaMemcpyHostToDevice, h->stream), "upload pixels");
     }
-    ck(cudaStreamSynchronize(h->stream), "probe upload");  // host vectors go out of scope
+    ck(lbm::stream_wait(h->stream, h->timeout_s), "probe upload");  // host vectors go out of scope
     ck(cudaMallocHost(&h->hist_host, HIST_CAP * 8 * 8), "cudaMallocHost");
     h->mass_d = (double *)h->dalloc((2 + 2 * (size_t)lbm27::mass27_blocks()) * sizeof(double) + 16);
     ck(cudaMemset(h->mass_d, 0, (2 + 2 * (size_t)lbm27::mass27_blocks()) * sizeof(double) + 16), "memset");

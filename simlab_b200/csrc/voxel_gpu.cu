@@ -36,6 +36,7 @@
 #include <string>
 #include <vector>
 
+#include "host_wait.hpp"
 #include "voxel.hpp"
 
 namespace lbm {
@@ -401,6 +402,8 @@ struct Pool {
     }
 };
 
+constexpr double VOXEL_WAIT_S = 600.0;  // host-side limit on each wait for the voxelizer's kernels
+
 unsigned blocks(uint64_t n) { return (unsigned)((n + vg::T - 1) / vg::T); }
 
 // offs[0..n] = exclusive prefix sum of count[0..n-1] (count has n + 1
@@ -409,7 +412,7 @@ uint64_t scan(cudaStream_t st, const uint32_t *count, uint64_t *offs, uint64_t n
     thrust::exclusive_scan(thrust::cuda::par.on(st), count, count + n + 1, offs, (uint64_t)0);
     uint64_t tot = 0;
     ck(cudaMemcpyAsync(&tot, offs + n, 8, cudaMemcpyDeviceToHost, st), "scan total");
-    ck(cudaStreamSynchronize(st), "scan");
+    ck(lbm::stream_wait(st, VOXEL_WAIT_S), "scan");
     return tot;
 }
 
@@ -421,7 +424,7 @@ struct NonZero {
 uint32_t select_idx(cudaStream_t st, const uint32_t *flag, uint64_t n, uint32_t *out) {
     auto end = thrust::copy_if(thrust::cuda::par.on(st), thrust::counting_iterator<uint32_t>(0), thrust::counting_iterator<uint32_t>((uint32_t)n), flag,
                                out, NonZero());
-    ck(cudaStreamSynchronize(st), "select");
+    ck(lbm::stream_wait(st, VOXEL_WAIT_S), "select");
     return (uint32_t)(end - out);
 }
 
@@ -467,7 +470,9 @@ StaticVoxels voxelize_static_gpu(const Surface &s, std::array<size_t, 3> dims, i
     ck(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking), "cudaStreamCreate");
     struct StreamGuard {
         cudaStream_t s;
-        ~StreamGuard() { cudaStreamSynchronize(s); cudaStreamDestroy(s); }
+        ~StreamGuard() {
+            if (lbm::stream_wait(s, VOXEL_WAIT_S) != cudaErrorTimeout) cudaStreamDestroy(s);
+        }
     } sg{st};
     Pool pool;
     // vertices (lattice units) and their region coordinates (the grid has
@@ -505,7 +510,7 @@ StaticVoxels voxelize_static_gpu(const Surface &s, std::array<size_t, 3> dims, i
         vg::kv_crossings<true><<<blocks(nt), vg::T, 0, st>>>(gv, tris, nt, a, R, count, offs, hts, hws);
         vg::kv_lines<<<blocks(nlines), vg::T, 0, st>>>(a, R, count, offs, hts, hws, votes);
         ck(cudaGetLastError(), "scan lines");
-        ck(cudaStreamSynchronize(st), "scan lines");
+        ck(lbm::stream_wait(st, VOXEL_WAIT_S), "scan lines");
     }
     vg::kv_inside<<<blocks(glen), vg::T, 0, st>>>(glen, votes, inside);
     ck(cudaGetLastError(), "inside");
@@ -547,7 +552,7 @@ StaticVoxels voxelize_static_gpu(const Surface &s, std::array<size_t, 3> dims, i
     ck(cudaGetLastError(), "thin links");
     uint32_t herr = 0;
     ck(cudaMemcpyAsync(&herr, err, 4, cudaMemcpyDeviceToHost, st), "readback");
-    ck(cudaStreamSynchronize(st), "links");
+    ck(lbm::stream_wait(st, VOXEL_WAIT_S), "links");
     if (herr) throw VoxelError(1, "GPU voxelizer: a thin-sheet link reached a cell outside the candidate set");
 
     // walls and solid cells in region order, to the host
@@ -568,7 +573,7 @@ StaticVoxels voxelize_static_gpu(const Surface &s, std::array<size_t, 3> dims, i
     static_assert(sizeof(vg::WallRec) == sizeof(WallCell), "wall record layout");
     if (ns) ck(cudaMemcpyAsync(out.solid.data(), solid, (size_t)ns * 4, cudaMemcpyDeviceToHost, st), "readback");
     if (nw) ck(cudaMemcpyAsync(out.walls.data(), wrec, (size_t)nw * sizeof(WallCell), cudaMemcpyDeviceToHost, st), "readback");
-    ck(cudaStreamSynchronize(st), "readback");
+    ck(lbm::stream_wait(st, VOXEL_WAIT_S), "readback");
     return out;
 }
 
