@@ -322,6 +322,7 @@ def test_gpu_periodic_sphere_array_stokes_drag():
     c = 4.0 / 3.0 * np.pi * r ** 3 / vol
     k_ref = 1.0 / (1.0 - 1.7601 * c ** (1 / 3) + c - 1.5593 * c * c + 3.9799 * c ** (8 / 3) - 3.0734 * c ** (10 / 3))
     k = f / (6.0 * np.pi * nu * r * ux)
+    print(f"periodic sphere array: K {k:.4f} vs {k_ref:.4f} ({(k / k_ref - 1) * 100:+.2f} %)")
     assert abs(k / k_ref - 1.0) < 0.04, (k, k_ref)
 
 
