@@ -684,6 +684,13 @@ def _window_check(w: np.ndarray, p: Plan, axis_l: np.ndarray):
     nbk = 8
     bl = len(w) // nbk
     xs = np.arange(nbk) - (nbk - 1) / 2.0
+    if bl == 0:  # fewer samples than blocks: no block statistics (the reference's 0/0 gives no trend and no error)
+        for s in sigs:
+            m1, m2 = s[:half].mean(), s[half:].mean()
+            sc = 0.5 * (abs(m1) + abs(m2))
+            if sc > 0.0:
+                worst = max(worst, abs(m2 - m1) / 2.0 / sc)
+        return worst, se_rel, trend, half
     for s in sigs:
         m1, m2 = s[:half].mean(), s[half:].mean()
         sc = 0.5 * (abs(m1) + abs(m2))
