@@ -203,6 +203,29 @@ def test_zero_steps_change_nothing():
     assert g.save_state() == blob
 
 
+def test_profile_modes():
+    """lbm_profile: mode 1 times faces, walls and bulk; mode 2 only the bulk
+    kernel (faces and walls read 0); both count the engine's launches; other
+    modes are refused.  Profiling changes no result."""
+    st, vox = sphere_re40(Storage.FP16)
+    a, b = Lattice(st, vox), Lattice(st, vox)
+    a.advance(4)
+    b.advance(4)
+    a.profile(2)
+    fa = a.run(10)
+    k2 = a.kernel_times()
+    assert k2["steps"] == 10 and k2["faces_ms"] == 0.0 and k2["walls_ms"] == 0.0 and k2["bulk_ms"] > 0.0 and k2["launches"] >= 10
+    a.profile(1)
+    a.advance(10)
+    k1 = a.kernel_times()
+    assert k1["steps"] == 10 and k1["faces_ms"] > 0.0 and k1["bulk_ms"] > 0.0 and k1["launches"] == k2["launches"]
+    a.profile(0)
+    with pytest.raises(LbmError):
+        a.profile(3)
+    fb = b.run(10)
+    assert np.array_equal(fa, fb)
+
+
 def test_macros_needs_debug_dump():
     st, vox = feature_case()
     st.debug_dump = False
