@@ -69,6 +69,7 @@ struct LevelParams {
     // wall records (finest level only; nrec = 0 elsewhere)
     uint32_t *recs;
     double *recd;               // FP64 engine: 6 doubles (F, T) per record
+    void *wallf;                // R, 27 per record: the wall populations the step substitutes
     uint32_t nrec;
     float4 *dump;
     // a spinning part on this (finest) level: every swept-box cell is a

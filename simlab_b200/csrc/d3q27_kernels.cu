@@ -304,15 +304,15 @@ __device__ __forceinline__ void gauss_raw(const R *u, const R *sg, const R *m1, 
         }
 }
 
-// Register budget (blocks of 256 threads per SM): FP32/FP16/BF16 without
-// periodic wrap run 3 (80 registers, a few spilled to L1), with wrap 2; the
-// FP64 engine (a validation instrument) keeps the compiler's choice.
-// Blocks per SM the step kernel is compiled for.  Without periodic axes and
-// sponges, 2-byte storage runs four blocks (64 registers, a few words
-// spilled; measured +6 % on the three-level lattice); FP32, and the sponge
-// variants, lose more to the spills than they gain and run three.
+// Blocks of 256 threads per SM the step kernel is compiled for.  With the
+// wall arithmetic in its own kernel, FP32, FP16 and BF16 fit 64 registers
+// without spilling when the level has neither periodic axes nor sponges, so
+// those run four blocks; sponges (the viscosity ramp and the absorbing
+// layer) need 80 registers and run three, periodic wrap (offsets per thread)
+// three, and both two.  The FP64 engine (a validation instrument) keeps the
+// compiler's choice.
 template <class S, bool WRAP, bool SPONGE> struct StepOcc {
-    static constexpr int value = WRAP ? 2 : ((sizeof(S) == 2 && !SPONGE) ? 4 : 3);
+    static constexpr int value = WRAP ? (SPONGE ? 2 : 3) : (SPONGE ? 3 : 4);
 };
 template <bool WRAP, bool SPONGE> struct StepOcc<double, WRAP, SPONGE> { static constexpr int value = 1; };
 
@@ -330,64 +330,16 @@ __device__ __forceinline__ void cell27(const LevelParams &p, const StepArgs &a, 
     using R = typename Pop<S>::real;
     const Consts27<R> &k = K<R>(p);
     const R SC = (R)Raw<S>::SC, ISC = (R)1 / (R)Raw<S>::SC;
-    const S *srcn = set_ptr<S>(p, a.src) + n;
     const int64_t NP = (int64_t)p.NP;
     const uint32_t rec = fg >> 3;
     if (rec != 0) {
-        // Bouzidi bounce-back with moving-wall momentum exchange (mshader.rs:364-403)
+        // the wall populations k27_walls computed for this cell this step
         const uint32_t r = rec - 1;
         const uint32_t mask = p.recs[r * RS + R_MASK];
-        R fin[27];
+        const R *wf = (const R *)p.wallf + (uint64_t)r * 27;
 #pragma unroll
-        for (int i = 0; i < 27; i++) fin[i] = f[i] * ISC;
-        R Fv[3] = {0, 0, 0}, Tv[3] = {0, 0, 0};
-        const R pc[3] = {(R)(float)x - k.center[0], (R)(float)y - k.center[1], (R)(float)z - k.center[2]};
-        R om[3];
-        if (sizeof(R) == 8) { om[0] = (R)a.omega_d[0]; om[1] = (R)a.omega_d[1]; om[2] = (R)a.omega_d[2]; }
-        else { om[0] = (R)a.omega[0]; om[1] = (R)a.omega[1]; om[2] = (R)a.omega[2]; }
-#pragma unroll
-        for (int i = 0; i < 27; i++) {
-            if (i == 13) continue;
-            if (!(mask & (1u << i))) continue;
-            const int o = 26 - i;
-            const uint32_t wq = p.recs[r * RS + R_Q + SLOT(i) / 2];
-            const uint16_t hq = (SLOT(i) & 1) ? (uint16_t)(wq >> 16) : (uint16_t)(wq & 0xffffu);
-            const R q = max((R)__half2float(__ushort_as_half(hq)), (R)0.001f);
-            const R fpi = Raw<S>::ld(srcn + (int64_t)i * NP) * ISC + W<R>(i);
-            const R fpo = Raw<S>::ld(srcn + (int64_t)o * NP) * ISC + W<R>(i);
-            const R ci[3] = {(R)CX(i), (R)CY(i), (R)CZ(i)};
-            const R xw[3] = {pc[0] + q * ci[0], pc[1] + q * ci[1], pc[2] + q * ci[2]};
-            const R uw[3] = {om[1] * xw[2] - om[2] * xw[1], om[2] * xw[0] - om[0] * xw[2], om[0] * xw[1] - om[1] * xw[0]};
-            const R cu = ci[0] * uw[0] + ci[1] * uw[1] + ci[2] * uw[2];
-            const R w6 = (R)6 * W<R>(i);
-            R fb;
-            if (q >= (R)0.5) fb = (fpi + ((R)2 * q - (R)1) * fpo - w6 * cu) / ((R)2 * q);
-            else if (!(mask & (1u << o))) fb = (R)2 * q * fpi + ((R)1 - (R)2 * q) * (fin[i] + W<R>(i)) - w6 * cu;
-            else fb = fpi - w6 * cu;
-            f[o] = (fb - W<R>(i)) * SC;
-            R flk[3];
-#pragma unroll
-            for (int c = 0; c < 3; c++) flk[c] = (ci[c] - uw[c]) * fpi + (ci[c] + uw[c]) * fb;
-#pragma unroll
-            for (int c = 0; c < 3; c++) Fv[c] += flk[c];
-            Tv[0] += xw[1] * flk[2] - xw[2] * flk[1];
-            Tv[1] += xw[2] * flk[0] - xw[0] * flk[2];
-            Tv[2] += xw[0] * flk[1] - xw[1] * flk[0];
-        }
-        if (p.moving) {
-            // plus what the re-voxelizer booked for this cell this step
-            for (int c = 0; c < 3; c++) {
-                Fv[c] += p.recd ? (R)p.recd[r * 6 + c] : (R)__uint_as_float(p.recs[r * RS + R_FT + c]);
-                Tv[c] += p.recd ? (R)p.recd[r * 6 + 3 + c] : (R)__uint_as_float(p.recs[r * RS + R_FT + 3 + c]);
-            }
-        }
-        for (int c = 0; c < 3; c++) {
-            p.recs[r * RS + R_FT + c] = __float_as_uint((float)Fv[c]);
-            p.recs[r * RS + R_FT + 3 + c] = __float_as_uint((float)Tv[c]);
-        }
-        if (p.recd) {
-            for (int c = 0; c < 3; c++) { p.recd[r * 6 + c] = (double)Fv[c]; p.recd[r * 6 + 3 + c] = (double)Tv[c]; }
-        }
+        for (int i = 0; i < 27; i++)
+            if (i != 13 && (mask & (1u << i))) f[26 - i] = wf[26 - i];
     }
     Mom<R> mo = moments<R>(f);
     if (Raw<S>::SC != 1) {
@@ -491,6 +443,94 @@ __device__ __forceinline__ void cell27(const LevelParams &p, const StepArgs &a, 
     }
 }
 
+
+// Bouzidi bounce-back with moving-wall momentum exchange (mshader.rs:364-403),
+// one thread per wall record, launched just before the step on the same
+// stream.  For each cut link i of a cell the step will update, the
+// population the step takes instead of the one it pulls from the solid side
+// (direction 26 - i, storage units) goes to wallf, 27 slots per record; the
+// force and moment on the wall go to the record.  Kept out of the step, the
+// wall arithmetic (and the pulled values it needs next to the substituted
+// ones) no longer shares the collision's register budget: the step compiled
+// for four blocks per SM spilled with it inline.
+template <class S>
+__global__ void __launch_bounds__(BLK) k27_walls(const __grid_constant__ LevelParams p, const StepArgs a) {
+    using R = typename Pop<S>::real;
+    const uint32_t r = blockIdx.x * BLK + threadIdx.x;
+    if (r >= p.nrec) return;
+    const uint32_t n = p.recs[r * RS + R_CELL];
+    const uint32_t fg = p.flags[n];
+    // only the cells the step updates, each through its own record
+    if ((fg & 7u) != 0 || (fg >> 3) != r + 1) return;
+    uint32_t x, y, z;
+    coords(p, n, x, y, z);
+    const Consts27<R> &k = K<R>(p);
+    const R SC = (R)Raw<S>::SC, ISC = (R)1 / (R)Raw<S>::SC;
+    const S *srcn = set_ptr<S>(p, a.src) + n;
+    const int64_t NP = (int64_t)p.NP;
+    // the step's pull offsets (with periodic wrap where an axis has it; a
+    // stepped cell of a closed axis is never on its edge)
+    const int32_t nx = (int32_t)p.NX, nxy = (int32_t)(p.NX * p.NY);
+    const int32_t xo[3] = {x == 0 ? nx - 1 : -1, 0, x == p.NX - 1 ? -(nx - 1) : 1};
+    const int32_t yo[3] = {y == 0 ? (int32_t)(p.NY - 1) * nx : -nx, 0, y == p.NY - 1 ? -(int32_t)(p.NY - 1) * nx : nx};
+    const int32_t zo[3] = {z == 0 ? (int32_t)(p.NZ - 1) * nxy : -nxy, 0, z == p.NZ - 1 ? -(int32_t)(p.NZ - 1) * nxy : nxy};
+    const uint32_t mask = p.recs[r * RS + R_MASK];
+    R *wf = (R *)p.wallf + (uint64_t)r * 27;
+    R Fv[3] = {0, 0, 0}, Tv[3] = {0, 0, 0};
+    const R pc[3] = {(R)(float)x - k.center[0], (R)(float)y - k.center[1], (R)(float)z - k.center[2]};
+    R om[3];
+    if (sizeof(R) == 8) { om[0] = (R)a.omega_d[0]; om[1] = (R)a.omega_d[1]; om[2] = (R)a.omega_d[2]; }
+    else { om[0] = (R)a.omega[0]; om[1] = (R)a.omega[1]; om[2] = (R)a.omega[2]; }
+#pragma unroll
+    for (int i = 0; i < 27; i++) {
+        if (i == 13) continue;
+        if (!(mask & (1u << i))) continue;
+        const int o = 26 - i;
+        const uint32_t wq = p.recs[r * RS + R_Q + SLOT(i) / 2];
+        const uint16_t hq = (SLOT(i) & 1) ? (uint16_t)(wq >> 16) : (uint16_t)(wq & 0xffffu);
+        const R q = max((R)__half2float(__ushort_as_half(hq)), (R)0.001f);
+        const R fpi = Raw<S>::ld(srcn + (int64_t)i * NP) * ISC + W<R>(i);
+        const R fpo = Raw<S>::ld(srcn + (int64_t)o * NP) * ISC + W<R>(i);
+        const R ci[3] = {(R)CX(i), (R)CY(i), (R)CZ(i)};
+        const R xw[3] = {pc[0] + q * ci[0], pc[1] + q * ci[1], pc[2] + q * ci[2]};
+        const R uw[3] = {om[1] * xw[2] - om[2] * xw[1], om[2] * xw[0] - om[0] * xw[2], om[0] * xw[1] - om[1] * xw[0]};
+        const R cu = ci[0] * uw[0] + ci[1] * uw[1] + ci[2] * uw[2];
+        const R w6 = (R)6 * W<R>(i);
+        R fb;
+        if (q >= (R)0.5) {
+            fb = (fpi + ((R)2 * q - (R)1) * fpo - w6 * cu) / ((R)2 * q);
+        } else if (!(mask & (1u << o))) {
+            // the population pulled along c_i, as the step loads it
+            const R fin = Raw<S>::ld(srcn + ((int64_t)i * NP + (xo[1 - CX(i)] + yo[1 - CY(i)] + zo[1 - CZ(i)]))) * ISC;
+            fb = (R)2 * q * fpi + ((R)1 - (R)2 * q) * (fin + W<R>(i)) - w6 * cu;
+        } else {
+            fb = fpi - w6 * cu;
+        }
+        wf[o] = (fb - W<R>(i)) * SC;
+        R flk[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) flk[c] = (ci[c] - uw[c]) * fpi + (ci[c] + uw[c]) * fb;
+#pragma unroll
+        for (int c = 0; c < 3; c++) Fv[c] += flk[c];
+        Tv[0] += xw[1] * flk[2] - xw[2] * flk[1];
+        Tv[1] += xw[2] * flk[0] - xw[0] * flk[2];
+        Tv[2] += xw[0] * flk[1] - xw[1] * flk[0];
+    }
+    if (p.moving) {
+        // plus what the re-voxelizer booked for this cell this step
+        for (int c = 0; c < 3; c++) {
+            Fv[c] += p.recd ? (R)p.recd[r * 6 + c] : (R)__uint_as_float(p.recs[r * RS + R_FT + c]);
+            Tv[c] += p.recd ? (R)p.recd[r * 6 + 3 + c] : (R)__uint_as_float(p.recs[r * RS + R_FT + 3 + c]);
+        }
+    }
+    for (int c = 0; c < 3; c++) {
+        p.recs[r * RS + R_FT + c] = __float_as_uint((float)Fv[c]);
+        p.recs[r * RS + R_FT + 3 + c] = __float_as_uint((float)Tv[c]);
+    }
+    if (p.recd) {
+        for (int c = 0; c < 3; c++) { p.recd[r * 6 + c] = (double)Fv[c]; p.recd[r * 6 + 3 + c] = (double)Tv[c]; }
+    }
+}
 
 template <class S, bool FORCE, bool WRAP, bool SPONGE>
 __global__ void __launch_bounds__(BLK, StepOcc<S, WRAP, SPONGE>::value) k27_step(const __grid_constant__ LevelParams p, const StepArgs a) {
@@ -1029,6 +1069,7 @@ cudaError_t launch27_step(int storage, const LevelParams &p, const StepArgs &a, 
         const bool wrap = p.per[0] || p.per[1] || p.per[2];
         const unsigned g = blocks_for(p.N);
         const bool sp = p.n_sponge != 0;
+        if (p.nrec) k27_walls<S><<<blocks_for(p.nrec), BLK, 0, st>>>(p, a);
         if (p.forcing) {
             if (wrap) {
                 if (sp) k27_step<S, true, true, true><<<g, BLK, 0, st>>>(p, a);

@@ -82,6 +82,7 @@ struct lbm_multi {
     uint32_t nrec = 0;
     uint32_t *recs = nullptr;
     double *recd = nullptr;
+    void *wallf = nullptr;  // 27 reals per record, written by the wall kernel each finest step
     double *partials = nullptr;
     uint32_t *ticket = nullptr;
     double *hist = nullptr;       // HIST_CAP x 8 doubles
@@ -537,6 +538,7 @@ void create_multi(const lbm_multi_setup *setup, const lbm_geometry *geom, const 
         h->recd = (double *)h->dalloc(std::max<uint64_t>(nrec, 1) * 6 * 8);
         ck(cudaMemsetAsync(h->recd, 0, std::max<uint64_t>(nrec, 1) * 6 * 8, h->stream), "records init");
     }
+    h->wallf = h->dalloc(std::max<uint64_t>(nrec, 1) * 27 * rsz);
     h->partials = (double *)h->dalloc((size_t)std::max<uint32_t>(lbm27::reduce27_blocks(h->nrec), 1) * 8 * 8);
     h->ticket = (uint32_t *)h->dalloc(16);
     ck(cudaMemsetAsync(h->ticket, 0, 16, h->stream), "ticket init");
@@ -584,8 +586,8 @@ void create_multi(const lbm_multi_setup *setup, const lbm_geometry *geom, const 
     for (size_t l = 0; l < nl; l++) {
         lbm27::LevelParams &p = h->lv[l].p;
         p.dump = h->dump;
-        if (l == finest) { p.recs = h->recs; p.recd = h->recd; p.nrec = h->nrec; }
-        else { p.recs = nullptr; p.recd = nullptr; p.nrec = 0; }
+        if (l == finest) { p.recs = h->recs; p.recd = h->recd; p.wallf = h->wallf; p.nrec = h->nrec; }
+        else { p.recs = nullptr; p.recd = nullptr; p.wallf = nullptr; p.nrec = 0; }
         ck(lbm27::launch27_init(s.storage, p, h->stream), "init kernel");
     }
     h->wait();
