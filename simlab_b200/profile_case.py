@@ -19,6 +19,13 @@
     python -m simlab_b200.profile_case gray [steps]
         the gray-level design case (192x96x96, FP32): forward steps, then one
         adjoint sweep over the same steps (checkpoint every 10)
+    python -m simlab_b200.profile_case voxel [19|27]
+        the static voxelizer on the GPU: a sphere of radius 100 cells (81,920
+        triangles) in a 222^3 lattice, two calls
+    python -m simlab_b200.profile_case levelprobes [finest steps]
+        three D3Q27 levels (coarse 128x64x64, FP16) with a sphere of radius 12
+        on the finest, its surface vertices and two slices sampled every
+        finest step, then the mass of each level and the finest level's dump
 """
 from __future__ import annotations
 
@@ -96,9 +103,57 @@ def _gray(args) -> None:
     print(f"profile case gray: {steps} steps forward, adjoint objective {j:.6e}, |grad| {float((g * g).sum()) ** 0.5:.3e}")
 
 
+def _voxel(args) -> None:
+    from .lbm import voxelize_static
+    from .shapes import sphere
+
+    q = int(args[0]) if args else 19
+    v, t = sphere([110.3, 110.7, 110.1], 100.0, 6)
+    for _ in range(2):
+        vox = voxelize_static(v, t, [222] * 3, q, device=True)
+    print(f"profile case voxel D3Q{q}: {len(t)} triangles, {len(vox.solid)} solid cells, {len(vox.walls)} wall records")
+
+
+def _levelprobes(args) -> None:
+    import numpy as np
+
+    from .lbm import Probes, SliceDef, steps_array, voxelize_static
+    from .mlattice import LevelBox, MultiLattice, MultiSetup
+    from .shapes import sphere
+
+    steps = int(args[0]) if args else 8
+    F = FaceBc
+    s = MultiSetup(dims0=[128, 64, 64], faces=[F.VELOCITY] + [F.OPEN] * 5, nu0=0.001, u_inf=[0.05, 0, 0], u_init=[0.05, 0, 0],
+                   sponge=[0, 16, 8, 8, 8, 8], sponge_tau=1.0, sponge_sigma=0.1, total_pressure_inlet=True, storage=Storage.FP16,
+                   debug_dump=True)
+    for l in range(1, 3):
+        d = s.dims(l - 1)
+        n = [int(d[k] * 0.63) for k in range(3)]
+        s.boxes.append(LevelBox(lo=[(d[k] - n[k]) // 2 for k in range(3)], n=n))
+    fd = s.dims(2)
+    c = [fd[0] * 0.4 + 0.3, fd[1] * 0.5 + 0.2, fd[2] * 0.5 + 0.1]
+    s.center = c
+    v, t = sphere(c, 12.0, 4)
+    vox = voxelize_static(v, t, list(fd), 27)
+    rel = np.asarray(v) - np.asarray(c)
+    verts = [(tuple(p), tuple(p / np.linalg.norm(p))) for p in rel]
+    # slices in finest-level units over the whole domain: the finest level's
+    # node 0 sits at 4 lo(box 1) + 2 lo(box 2)
+    org = [4 * s.boxes[0].lo[k] + 2 * s.boxes[1].lo[k] for k in range(3)]
+    yc, zc = org[1] + int(round(c[1])), org[2] + int(round(c[2]))
+    slices = [SliceDef(origin=[0, 0, zc], u=[2, 0, 0], v=[0, 2, 0], nu=256, nv=128),
+              SliceDef(origin=[0, yc, 0], u=[2, 0, 0], v=[0, 0, 2], nu=256, nv=128)]
+    lat = MultiLattice(s, vox, probes=Probes(verts=verts, slices=slices, vertex_offset=0.5))
+    lat.run(steps_array(steps, sample=True))
+    masses = [lat.mass(l) for l in range(lat.levels)]
+    m = lat.macros(2)
+    print(f"profile case levelprobes {lat.level_cells()}: {steps} sampled finest steps, {lat.nvert} vertices, {lat.npix} pixels, "
+          f"masses {[f'{x[0]:.4e}' for x in masses]}, finest macros {m.shape}")
+
+
 def main() -> None:
     args = sys.argv[1:]
-    cases = {"levels": _levels, "spin": _spin, "probes": _probes, "gray": _gray}
+    cases = {"levels": _levels, "spin": _spin, "probes": _probes, "gray": _gray, "voxel": _voxel, "levelprobes": _levelprobes}
     if args and args[0] in cases:
         cases[args[0]](args[1:])
         return
