@@ -145,7 +145,7 @@ def _levelprobes(args) -> None:
               SliceDef(origin=[0, yc, 0], u=[2, 0, 0], v=[0, 0, 2], nu=256, nv=128)]
     lat = MultiLattice(s, vox, probes=Probes(verts=verts, slices=slices, vertex_offset=0.5))
     lat.run(steps_array(steps, sample=True))
-    masses = [lat.mass(l) for l in range(lat.levels)]
+    masses = [lat.mass(l) for l in range(lat.levels())]
     m = lat.macros(2)
     print(f"profile case levelprobes {lat.level_cells()}: {steps} sampled finest steps, {lat.nvert} vertices, {lat.npix} pixels, "
           f"masses {[f'{x[0]:.4e}' for x in masses]}, finest macros {m.shape}")
