@@ -453,8 +453,13 @@ __device__ __forceinline__ void cell27(const LevelParams &p, const StepArgs &a, 
 // wall arithmetic (and the pulled values it needs next to the substituted
 // ones) no longer shares the collision's register budget: the step compiled
 // for four blocks per SM spilled with it inline.
+// three blocks per SM: 80 registers hold the preloaded populations and link
+// distances without spilling (FP64 keeps the compiler's choice)
+template <class S> struct WallOcc { static constexpr int value = 3; };
+template <> struct WallOcc<double> { static constexpr int value = 1; };
+
 template <class S>
-__global__ void __launch_bounds__(BLK) k27_walls(const __grid_constant__ LevelParams p, const StepArgs a) {
+__global__ void __launch_bounds__(BLK, WallOcc<S>::value) k27_walls(const __grid_constant__ LevelParams p, const StepArgs a) {
     using R = typename Pop<S>::real;
     const uint32_t r = blockIdx.x * BLK + threadIdx.x;
     if (r >= p.nrec) return;
@@ -481,40 +486,55 @@ __global__ void __launch_bounds__(BLK) k27_walls(const __grid_constant__ LevelPa
     R om[3];
     if (sizeof(R) == 8) { om[0] = (R)a.omega_d[0]; om[1] = (R)a.omega_d[1]; om[2] = (R)a.omega_d[2]; }
     else { om[0] = (R)a.omega[0]; om[1] = (R)a.omega[1]; om[2] = (R)a.omega[2]; }
+    if (mask != 0u) {
+        // the link distances and the cell's own populations on the cut links
+        // (both ends) first, all independent: loaded inside each link's
+        // arithmetic, after the previous link's store (which the compiler
+        // cannot tell from them), the links' memory latencies ran one after
+        // another.  The pulled population, needed only by a short link whose
+        // opposite is open, is still loaded where it is used.
+        uint32_t qw[13];
 #pragma unroll
-    for (int i = 0; i < 27; i++) {
-        if (i == 13) continue;
-        if (!(mask & (1u << i))) continue;
-        const int o = 26 - i;
-        const uint32_t wq = p.recs[r * RS + R_Q + SLOT(i) / 2];
-        const uint16_t hq = (SLOT(i) & 1) ? (uint16_t)(wq >> 16) : (uint16_t)(wq & 0xffffu);
-        const R q = max((R)__half2float(__ushort_as_half(hq)), (R)0.001f);
-        const R fpi = Raw<S>::ld(srcn + (int64_t)i * NP) * ISC + W<R>(i);
-        const R fpo = Raw<S>::ld(srcn + (int64_t)o * NP) * ISC + W<R>(i);
-        const R ci[3] = {(R)CX(i), (R)CY(i), (R)CZ(i)};
-        const R xw[3] = {pc[0] + q * ci[0], pc[1] + q * ci[1], pc[2] + q * ci[2]};
-        const R uw[3] = {om[1] * xw[2] - om[2] * xw[1], om[2] * xw[0] - om[0] * xw[2], om[0] * xw[1] - om[1] * xw[0]};
-        const R cu = ci[0] * uw[0] + ci[1] * uw[1] + ci[2] * uw[2];
-        const R w6 = (R)6 * W<R>(i);
-        R fb;
-        if (q >= (R)0.5) {
-            fb = (fpi + ((R)2 * q - (R)1) * fpo - w6 * cu) / ((R)2 * q);
-        } else if (!(mask & (1u << o))) {
-            // the population pulled along c_i, as the step loads it
-            const R fin = Raw<S>::ld(srcn + ((int64_t)i * NP + (xo[1 - CX(i)] + yo[1 - CY(i)] + zo[1 - CZ(i)]))) * ISC;
-            fb = (R)2 * q * fpi + ((R)1 - (R)2 * q) * (fin + W<R>(i)) - w6 * cu;
-        } else {
-            fb = fpi - w6 * cu;
+        for (int w = 0; w < 13; w++) qw[w] = p.recs[r * RS + R_Q + w];
+        R own[27];
+#pragma unroll
+        for (int i = 0; i < 27; i++)
+            own[i] = (i != 13 && (mask & ((1u << i) | (1u << (26 - i))))) ? (R)Raw<S>::ld(srcn + (int64_t)i * NP) : (R)0;
+#pragma unroll
+        for (int i = 0; i < 27; i++) {
+            if (i == 13) continue;
+            if (!(mask & (1u << i))) continue;
+            const int o = 26 - i;
+            const uint32_t wq = qw[SLOT(i) / 2];
+            const uint16_t hq = (SLOT(i) & 1) ? (uint16_t)(wq >> 16) : (uint16_t)(wq & 0xffffu);
+            const R q = max((R)__half2float(__ushort_as_half(hq)), (R)0.001f);
+            const R fpi = own[i] * ISC + W<R>(i);
+            const R fpo = own[o] * ISC + W<R>(i);
+            const R ci[3] = {(R)CX(i), (R)CY(i), (R)CZ(i)};
+            const R xw[3] = {pc[0] + q * ci[0], pc[1] + q * ci[1], pc[2] + q * ci[2]};
+            const R uw[3] = {om[1] * xw[2] - om[2] * xw[1], om[2] * xw[0] - om[0] * xw[2], om[0] * xw[1] - om[1] * xw[0]};
+            const R cu = ci[0] * uw[0] + ci[1] * uw[1] + ci[2] * uw[2];
+            const R w6 = (R)6 * W<R>(i);
+            R fb;
+            if (q >= (R)0.5) {
+                fb = (fpi + ((R)2 * q - (R)1) * fpo - w6 * cu) / ((R)2 * q);
+            } else if (!(mask & (1u << o))) {
+                // the population pulled along c_i, as the step loads it
+                const R fin = Raw<S>::ld(srcn + ((int64_t)i * NP + (xo[1 - CX(i)] + yo[1 - CY(i)] + zo[1 - CZ(i)]))) * ISC;
+                fb = (R)2 * q * fpi + ((R)1 - (R)2 * q) * (fin + W<R>(i)) - w6 * cu;
+            } else {
+                fb = fpi - w6 * cu;
+            }
+            wf[o] = (fb - W<R>(i)) * SC;
+            R flk[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) flk[c] = (ci[c] - uw[c]) * fpi + (ci[c] + uw[c]) * fb;
+#pragma unroll
+            for (int c = 0; c < 3; c++) Fv[c] += flk[c];
+            Tv[0] += xw[1] * flk[2] - xw[2] * flk[1];
+            Tv[1] += xw[2] * flk[0] - xw[0] * flk[2];
+            Tv[2] += xw[0] * flk[1] - xw[1] * flk[0];
         }
-        wf[o] = (fb - W<R>(i)) * SC;
-        R flk[3];
-#pragma unroll
-        for (int c = 0; c < 3; c++) flk[c] = (ci[c] - uw[c]) * fpi + (ci[c] + uw[c]) * fb;
-#pragma unroll
-        for (int c = 0; c < 3; c++) Fv[c] += flk[c];
-        Tv[0] += xw[1] * flk[2] - xw[2] * flk[1];
-        Tv[1] += xw[2] * flk[0] - xw[0] * flk[2];
-        Tv[2] += xw[0] * flk[1] - xw[1] * flk[0];
     }
     if (p.moving) {
         // plus what the re-voxelizer booked for this cell this step
