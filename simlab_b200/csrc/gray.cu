@@ -261,10 +261,18 @@ __device__ __forceinline__ void step_cell(const GParams &p, const S *__restrict_
     }
 }
 
+// Forward steps are launched with programmatic stream serialization: every
+// block lets the next step's grid launch as soon as it starts, and waits for
+// the previous step's grid to complete (memory included) before it touches
+// global memory, so the next grid's blocks fill the SMs this grid's last wave
+// leaves free instead of starting after a launch gap.  Without the launch
+// attribute both instructions do nothing.
 template <class S, bool MOM, bool FORCE>
 __global__ void __launch_bounds__(BLK, 4) kg_step(const __grid_constant__ GParams p, const S *__restrict__ src, S *__restrict__ dst,
                                                typename GS<S>::R *__restrict__ mom, double *partials, uint32_t *ticket, double *out,
                                                uint32_t seed_mix) {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const uint32_t n = blockIdx.x * BLK + threadIdx.x;
     double fm[6] = {0, 0, 0, 0, 0, 0};
     if (n < p.N) step_cell<S, MOM, FORCE>(p, src, dst, mom, seed_mix, n, fm);
@@ -279,6 +287,9 @@ __global__ void __launch_bounds__(BLK, 4) kg_step(const __grid_constant__ GParam
 template <class R>
 __global__ void __launch_bounds__(BLK) kg_adjoint(const __grid_constant__ GParams p, const R *__restrict__ lin, R *__restrict__ lout,
                                                   const R *__restrict__ mom, double *__restrict__ grad, int objective, R swin) {
+    // launched like the forward steps (programmatic stream serialization)
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const uint32_t n = blockIdx.x * BLK + threadIdx.x;
     if (n >= p.N) return;
     uint32_t x, y, z;
@@ -447,10 +458,24 @@ struct lbm_gray {
             const uint32_t mix = seed_mix();
             const S *src = (const S *)P[cur];
             S *dst = (S *)P[1 - cur];
-            if (mom_slot && out) gray::kg_step<S, true, true><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, (R *)mom_slot, partials, ticket, out, mix);
-            else if (mom_slot) gray::kg_step<S, true, false><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, (R *)mom_slot, nullptr, nullptr, nullptr, mix);
-            else if (out) gray::kg_step<S, false, true><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, nullptr, partials, ticket, out, mix);
-            else gray::kg_step<S, false, false><<<nblk(), gray::BLK, 0, stream>>>(p, src, dst, nullptr, nullptr, nullptr, nullptr, mix);
+            // programmatic stream serialization (the kernel's first lines say how it is used)
+            cudaLaunchConfig_t cfg{};
+            cfg.gridDim = dim3(nblk());
+            cfg.blockDim = dim3(gray::BLK);
+            cfg.dynamicSmemBytes = 0;
+            cfg.stream = stream;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+            at[0].val.programmaticStreamSerializationAllowed = 1;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            R *ms = (R *)mom_slot;
+            double *pt = out ? partials : nullptr;
+            uint32_t *tk = out ? ticket : nullptr;
+            if (mom_slot && out) ck(cudaLaunchKernelEx(&cfg, gray::kg_step<S, true, true>, p, src, dst, ms, pt, tk, out, mix), "step kernel");
+            else if (mom_slot) ck(cudaLaunchKernelEx(&cfg, gray::kg_step<S, true, false>, p, src, dst, ms, pt, tk, out, mix), "step kernel");
+            else if (out) ck(cudaLaunchKernelEx(&cfg, gray::kg_step<S, false, true>, p, src, dst, ms, pt, tk, out, mix), "step kernel");
+            else ck(cudaLaunchKernelEx(&cfg, gray::kg_step<S, false, false>, p, src, dst, ms, pt, tk, out, mix), "step kernel");
         });
         ck(cudaGetLastError(), "step kernel");
         cur = 1 - cur;
@@ -572,9 +597,19 @@ double lbm_gray::backward(const lbm_adjoint_spec &sp, double *grad_out) {
             const double sw = (s2 >= sp.t0 && s2 <= sp.t1) ? swin : 0.0;
             typed([&](auto *tp) {
                 using R = typename gray::GS<std::remove_pointer_t<decltype(tp)>>::R;
-                gray::kg_adjoint<R><<<nblk(), gray::BLK, 0, stream>>>(p, (const R *)L[lc], (R *)L[1 - lc], (const R *)mslot, grad, sp.objective, (R)sw);
+                cudaLaunchConfig_t cfg{};
+                cfg.gridDim = dim3(nblk());
+                cfg.blockDim = dim3(gray::BLK);
+                cfg.dynamicSmemBytes = 0;
+                cfg.stream = stream;
+                cudaLaunchAttribute at[1];
+                at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+                at[0].val.programmaticStreamSerializationAllowed = 1;
+                cfg.attrs = at;
+                cfg.numAttrs = 1;
+                ck(cudaLaunchKernelEx(&cfg, gray::kg_adjoint<R>, p, (const R *)L[lc], (R *)L[1 - lc], (const R *)mslot, grad, sp.objective, (R)sw),
+                   "adjoint kernel");
             });
-            ck(cudaGetLastError(), "adjoint kernel");
             lc = 1 - lc;
         }
         t_rev += elapsed();
